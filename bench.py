@@ -1,0 +1,447 @@
+"""REMC benchmark: replica-steps/s and pair-energies/s on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload batch64]
+                  [--impl ours|reference]
+
+One bench step = one replica-exchange block of the workload: every replica of
+every system advances `--block-steps` (default 1000) Metropolis steps in one
+persistent sweep launch, followed by one exchange round, replayed as a CUDA
+graph. `value` = replica-steps/s over the whole job (all ranks); inputs are
+resident in HBM. `e2e` = the same metric through the C ABI with host buffers:
+every step uploads the full replica state from host memory, runs one block and
+reads state and energies back. Multi-GPU runs are weak scaling: each rank
+advances its own independent batch (a different seed), with no collective on
+the data path.
+
+--impl reference times the reference's own CPU engine (oracle/_ref/
+REMCDockingCPU, compiled from the reference sources) on bounded samples of
+the same workload, written in the reference's config/PDB formats, with all
+host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic cost per pair evaluation (FMA = 2 FLOP): residue pair with
+# Kim-Hummer contact + Debye-Hueckel = 41 FLOP + 2 MUFU (rsqrt, ex2);
+# crowder pair = 26 FLOP + 1 MUFU (rsqrt). A dE pair is two evaluations.
+FLOP_RESIDUE_PAIR = 41
+FLOP_CROWDER_PAIR = 26
+MUFU_RESIDUE_PAIR = 2
+MUFU_CROWDER_PAIR = 1
+FP32_LANES_PER_SM = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="batch64",
+                    choices=["batch64", "crowded", "two_chain", "assembly"])
+    ap.add_argument("--block-steps", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=20,
+                    help="MC steps of the per-replica-launch comparison sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+             "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            t = [x.strip() for x in ln.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx.append(float(t[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, t[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference CPU
+def reference_exe():
+    from oracle import bindings as ob
+    return ob.REF_EXE if os.path.exists(ob.REF_EXE) else None
+
+
+def run_reference_sample(workload, systems, mc_steps: int, resteps: int, cores: int):
+    """Run the reference CPU engine on the given system indices concurrently
+    (one process per system, threads dividing the replica count). Returns
+    (replica_steps, seconds, threads_used, detail)."""
+    exe = reference_exe()
+    if exe is None:
+        raise RuntimeError("reference engine not built (oracle/_ref/REMCDockingCPU)")
+    from remcdockingsimulator_b200 import synth
+    work = tempfile.mkdtemp(prefix="remc_ref_")
+    procs = []
+    threads_used = 0
+    try:
+        per = []
+        for si in systems:
+            R = workload.n_replicas[si]
+            t = R
+            while t > 1 and (t > cores or R % t):
+                t -= 1
+            d = os.path.join(work, "sys%03d" % si)
+            cfg = synth.write_reference_inputs(workload, si, d, mc_steps, resteps, t)
+            per.append((si, d, cfg, t, R))
+        # as many concurrent processes as the cores allow
+        slots = max(1, cores // max(p[3] for p in per))
+        env = dict(os.environ)
+        env["LD_LIBRARY_PATH"] = "/usr/local/cuda/lib64:" + env.get("LD_LIBRARY_PATH", "")
+        t0 = time.perf_counter()
+        pending = list(per)
+        running = []
+        sim_ms = []
+        rsteps = 0
+        while pending or running:
+            while pending and len(running) < slots:
+                si, d, cfg, t, R = pending.pop(0)
+                p = subprocess.Popen([exe, "-f", cfg, "-t", str(t)], cwd=d, env=env,
+                                     stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+                running.append((p, R))
+                threads_used = max(threads_used, t * min(slots, len(per)))
+            for p, R in list(running):
+                if p.poll() is not None:
+                    out = p.stdout.read()
+                    if p.returncode != 0:
+                        raise RuntimeError("reference engine failed:\n" + out[-2000:])
+                    m = re.search(r"Simulation:\s+([0-9.]+) ms", out)
+                    if m:
+                        sim_ms.append(float(m.group(1)))
+                    rsteps += R * mc_steps
+                    running.remove((p, R))
+            time.sleep(0.01)
+        wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    return rsteps, wall, threads_used, {"sim_ms": sim_ms, "processes": len(systems),
+                                        "concurrent": slots}
+
+
+def reference_sample_plan(workload, seed: int):
+    import numpy as np
+    n = len(workload.systems)
+    rng = np.random.default_rng(seed + 777)
+    k = min(n, 8)
+    systems = sorted(rng.choice(n, size=k, replace=False).tolist())
+    pairs_per_step = sum(workload.systems[i].n_beads ** 2 / 2 for i in systems) / k
+    # ~28e6 pair evaluations/s per core for the reference E() (measured order)
+    mc = max(4, min(200, int(2.0e7 / max(pairs_per_step, 1.0))))
+    return systems, mc
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from remcdockingsimulator_b200 import synth
+    from remcdockingsimulator_b200.engine import Engine
+
+    w = synth.WORKLOADS[args.workload](args.seed + 1000 * rank)
+    eng = Engine(w.systems, w.n_replicas, w.params)
+    eng.set_replica_params(w.ladders, np.full(len(w.systems), w.translate_step, np.float32),
+                           np.full(len(w.systems), w.rotate_step))
+    eng.energy_full()
+    stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=torch.device("cuda", local))
+    n_inst = eng.n_inst
+    B = args.block_steps
+    seed = 20241203 + rank
+
+    # L2 flush buffer (> 126 MB L2), written between timed steps, outside the timing
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    step_ctr = 0
+    for _ in range(args.warmup):
+        eng.run(1, B, seed, step_ctr * B, step_ctr)
+        step_ctr += 1
+    eng.sync()
+    eng.reset_counters()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            starts[k].record(stream)
+        eng.run(1, B, seed, step_ctr * B, step_ctr)
+        step_ctr += 1
+        with torch.cuda.stream(stream):
+            ends[k].record(stream)
+            flush.fill_(float(k))
+    eng.sync()
+    barrier()
+    clk = clocks.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ev_res, ev_crowd = eng.pair_evaluations()
+    t_local = ms / 1000.0
+    t_max = t_local
+    if world > 1:
+        t = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    replica_steps = n_inst * B * args.steps * world
+    value = replica_steps / t_max
+    pair_evals = (ev_res + ev_crowd)
+    if world > 1:
+        t = torch.tensor([float(pair_evals)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        pair_evals_all = float(t.item())
+    else:
+        pair_evals_all = float(pair_evals)
+
+    # ---- roofline of the dominant kernel (the persistent sweep), timed alone
+    eng.reset_counters()
+    rs, re_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_roof = 3
+    with torch.cuda.stream(stream):
+        rs.record(stream)
+    for k in range(n_roof):
+        eng.sweep(B, seed + 1, (step_ctr + k) * B)
+    with torch.cuda.stream(stream):
+        re_.record(stream)
+    eng.sync()
+    sweep_ms = rs.elapsed_time(re_) / n_roof
+    r_res, r_crowd = eng.pair_evaluations()
+    flop_launch = (r_res * FLOP_RESIDUE_PAIR + r_crowd * FLOP_CROWDER_PAIR) / n_roof
+    mufu_launch = (r_res * MUFU_RESIDUE_PAIR + r_crowd * MUFU_CROWDER_PAIR) / n_roof
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except OSError:
+        pass
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    max_mhz = float(peaks.get("sm_max_mhz") or clk.get("sm_max_mhz") or 1965.0)
+    fp32_peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    achieved = flop_launch / (sweep_ms / 1000.0) / 1e12
+    roofline = {"bound": "fp32", "kernel": "sweep_kernel", "achieved": round(achieved, 3),
+                "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4),
+                "peak_source": "nominal FP32 FMA issue rate (%d SMs x 128 lanes x 2) at the "
+                               "measured max SM clock %.0f MHz (MEASURED_PEAKS.json has no FP32 "
+                               "figure); the kernel is FP32/MUFU-bound, not HBM or tensor" %
+                               (sm_count, max_mhz),
+                "flop_per_launch": flop_launch, "launch_ms": round(sweep_ms, 4),
+                "mufu_per_s": mufu_launch / (sweep_ms / 1000.0),
+                "traffic": None}
+    prof_traffic = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_traffic):
+        try:
+            with open(prof_traffic) as fh:
+                roofline["traffic"] = json.load(fh).get(args.workload)
+        except (OSError, ValueError):
+            pass
+
+    # ---- plain per-replica launches on a short sample (same trajectory rule)
+    plain = None
+    if args.plain_steps > 0:
+        ps, pe = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ps.record(stream)
+        eng.sweep_plain(args.plain_steps, seed + 2, 0)
+        with torch.cuda.stream(stream):
+            pe.record(stream)
+        eng.sync()
+        p_ms = ps.elapsed_time(pe)
+        plain_rate = n_inst * args.plain_steps / (p_ms / 1000.0) * world
+        plain = {"value": plain_rate, "unit": "replica-steps/s", "steps": args.plain_steps,
+                 "launches": n_inst * args.plain_steps,
+                 "batched_over_plain": value / plain_rate}
+
+    # ---- e2e through the C ABI with host buffers
+    st = eng.download_state()
+    host = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in st]
+    e2e_steps = max(2, min(args.steps, 5))
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        eng.upload_state(*host)
+        eng.run(1, B, seed + 3, k * B, k)
+        st2 = eng.download_state()
+        en = eng.energies()
+        for dst, src in zip(host, st2):
+            dst[...] = src
+    eng.sync()
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    h2d = sum(a.nbytes for a in host)
+    d2h = h2d + en.nbytes
+    e2e = {"value": n_inst * B * e2e_steps * world / t_e2e, "unit": "replica-steps/s",
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "path": "remc_upload_state + remc_run + remc_download_state + remc_get_energies"}
+
+    # ---- CPU baseline (reference engine, bounded sample), rank 0 at N = 1
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.seed)
+
+    gpu_launches = args.steps * 3  # per graph replay: sweep, exchange, counter advance
+    if rank == 0:
+        line = {
+            "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",
+            "value": value, "unit": "replica-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max * 1000.0 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded generator with the benchmark configuration's shapes)",
+            "config": {"workload": w.name, "description": w.description,
+                       "systems": len(w.systems), "replica_instances": n_inst,
+                       "beads_per_replica_mean": sum(s.n_beads * r for s, r in
+                                                     zip(w.systems, w.n_replicas)) / n_inst,
+                       "mc_steps_per_bench_step": B, "exchange_every": B,
+                       "l2": "256 MB buffer written between timed steps, outside the timing",
+                       "parallelism": "replicas" if world == 1 else "weak: %d independent batches" % world},
+            "pair_energies_per_s": pair_evals_all / t_max,
+            "pair_energy_note": "pair evaluations per second; a dE pair counts twice",
+            "roofline": roofline, "plain": plain, "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": clk, "gpu_launches": gpu_launches,
+        }
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(workload, seed: int):
+    cores = os.cpu_count() or 1
+    try:
+        systems, mc = reference_sample_plan(workload, seed)
+        rsteps, wall, threads, detail = run_reference_sample(workload, systems, mc, 2, cores)
+        return {"value": rsteps / wall, "unit": "replica-steps/s", "cores": threads,
+                "kind": "reference",
+                "sample": "reference REMCDockingCPU on %d of %d systems x all replicas x %d MC "
+                          "steps (full energy per step, its own (6/r)^6 crowder model and "
+                          "lambda=0.159), wall time incl. start-up" % (len(systems),
+                                                                    len(workload.systems), mc),
+                "detail": detail}
+    except Exception as exc:  # reported, not fatal: the GPU number stands alone
+        return {"value": None, "unit": "replica-steps/s", "cores": 0, "kind": "reference",
+                "sample": "failed: %s" % str(exc)[:300]}
+
+
+def reference_arm(args, world: int, rank: int):
+    if rank != 0:
+        return 0
+    from remcdockingsimulator_b200 import synth
+    exe = reference_exe()
+    if exe is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU engine not built in oracle/_ref"}))
+        return 0
+    w = synth.WORKLOADS[args.workload](args.seed)
+    cores = os.cpu_count() or 1
+    systems, mc = reference_sample_plan(w, args.seed)
+    for _ in range(args.warmup):
+        run_reference_sample(w, systems[:1], max(2, mc // 4), 1, cores)
+    total_rs = 0
+    total_t = 0.0
+    threads = 0
+    for _ in range(args.steps):
+        rs, wall, threads, detail = run_reference_sample(w, systems, mc, 2, cores)
+        total_rs += rs
+        total_t += wall
+    value = total_rs / total_t
+    line = {
+        "impl": "reference",
+        "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",
+        "value": value, "unit": "replica-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_t * 1000.0 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded generator, written in the reference's config/PDB formats)",
+        "config": {"workload": w.name, "description": w.description,
+                   "sample_systems": systems, "mc_steps_per_sample": mc},
+        "cpu_baseline": {"value": value, "unit": "replica-steps/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": "%d systems x all replicas x %d MC steps per bench step" %
+                                   (len(systems), mc)},
+        "e2e": {"value": value, "unit": "replica-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,160 @@
+/* remc_b200.h - C ABI of the B200 replica-exchange Monte Carlo docking engine.
+ *
+ * One handle holds many independent REMC systems (rigid residue-level chains
+ * and crowders in a periodic box), each with its own replicas, resident on one
+ * GPU. Every entry point returns an int status (REMC_OK = 0, negative on
+ * error; remc_last_error_string() gives the message). No entry point exits or
+ * aborts the process. A handle is not thread-safe: use one handle per host
+ * thread. All work is stream-ordered on a handle-owned CUDA stream.
+ *
+ * Counterparts in the reference (iantunbridge/RemcDockingSimulator, paths
+ * inside the project):
+ *   remc_energy_full ....... Replica::EonDevice / CUDA_EonDevice
+ *                            (simulation engine/src/Replica.cpp:1601-1616,
+ *                             CudaFunctions.cu:304-385) and Replica::E()
+ *                            (Replica.cpp:603-745)
+ *   remc_sweep ............. Replica::MCSearch (Replica.cpp:368-478), run for
+ *                            all replicas of all systems at once
+ *   remc_exchange .......... the exchange loop of REMCSimulation
+ *                            (main.cpp:1427-1453) + Replica::exchangeReplicas
+ *                            (Replica.cpp:145-159)
+ *   remc_upload_state ...... Replica::ReplicaDataToDevice (Replica.cpp:1308-1417)
+ *   remc_download_state .... Replica::ReplicaDataToHost (Replica.cpp:1433-1480)
+ *   remc_set_type_tables ... copyLJPotentialDataToDevice + bindLJTexture
+ *                            (CudaFunctions.cu:20-33, 112-131)
+ *   remc_set_params ........ the compile-time constants of definitions.h:11-35
+ *                            and CUDA_setBoxDimension (CudaFunctions.cu:169-174)
+ *   remc_delta_energy ...... no reference counterpart (the reference always
+ *                            recomputes the full energy); ΔE of one rigid move
+ */
+#ifndef REMC_B200_H
+#define REMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define REMC_OK 0
+#define REMC_ERR_INVALID (-1)   /* bad argument */
+#define REMC_ERR_CUDA (-2)      /* CUDA runtime error */
+#define REMC_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define REMC_ERR_STATE (-4)     /* call out of order (e.g. no state uploaded) */
+#define REMC_ERR_NUMERIC (-5)   /* non-finite input coordinates */
+#define REMC_ERR_TIMEOUT (-6)   /* a bounded device-side wait gave up */
+
+#define REMC_NUM_AMINO 20       /* residue types 0..19 */
+#define REMC_MAX_TYPES 24       /* 20 residue types + up to 4 crowder species */
+
+typedef struct remc_handle remc_handle;
+
+/* Energy model. Defaults (remc_default_params) are the reference's
+ * compile-time values (definitions.h:11-35, 89; Replica.cpp:624). */
+typedef struct {
+  float lambda_;        /* contact-energy scale lambda (0.159) */
+  float e0;             /* contact-energy offset e0 (-2.27) */
+  float debye_length;   /* Debye length Xi in Angstrom (10) */
+  float dh_const;       /* 0.948 * 1.602176487^2 */
+  float lj_cf;          /* LJ_CONVERSION_FACTOR 0.3507221006079 */
+  float kbt_cf;         /* KBTConversionFactor 1/(294 R/4184) */
+  int crowder_mode;     /* 0: (6/r)^6 (reference); 1: eps_c ((rho_i+rho_j)/r)^12 */
+  float crowder_cutoff; /* crowder pair cutoff in Angstrom (15); <= 0: none */
+  float crowder_eps;    /* eps_c, prefactor of the r^-12 crowder term */
+} remc_params;
+
+/* One system: topology shared by all of its replicas. Bead types 0..19 are
+ * residue types; types 20..23 are crowder species. A molecule is a crowder
+ * iff mol_role = -1; all beads of a crowder molecule must have crowder types,
+ * all beads of a chain residue types. */
+typedef struct {
+  int n_beads;
+  int n_mol;
+  int n_replicas;
+  const int* mol_start;   /* [n_mol + 1], mol_start[0] = 0, increasing */
+  const int* mol_role;    /* [n_mol]: 0 chain, -1 crowder */
+  const int* bead_type;   /* [n_beads] */
+  float box;              /* periodic box edge, Angstrom */
+  int translate_only_crowders; /* 1: crowders are never rotated */
+} remc_system_desc;
+
+void remc_default_params(remc_params* p);
+
+int remc_create(const remc_system_desc* systems, int n_systems, const remc_params* params,
+                remc_handle** out);
+int remc_destroy(remc_handle* h);
+int remc_set_params(remc_handle* h, const remc_params* params);
+
+/* Per-type tables (REMC_MAX_TYPES entries each): vdW radius (sigma_ij is the
+ * mean of the two radii), charge, crowder radius rho; raw pair table
+ * M[20*20] (eps_ab = lambda (M_ab - e0) evaluated in FP32, as the reference
+ * does at CudaFunctions.cu:581-594). */
+int remc_set_type_tables(remc_handle* h, const float* vdw, const float* charge, const float* rho,
+                         const float* pair_table_20x20);
+
+/* Instance layout: replica-instances are numbered system by system, slot by
+ * slot: inst = sum_{s' < s} R_s' + slot. Bead arrays are 3 floats per bead per
+ * instance in the same order; molecule arrays 3 floats (centre) or 4 doubles
+ * (quaternion w,x,y,z) per molecule per instance. */
+int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const float* centre,
+                      const double* quat);
+int remc_download_state(remc_handle* h, float* pos, float* rel, float* centre, double* quat);
+
+/* Temperature ladder per system (R floats per system, increasing, the
+ * instance order above), translate step (float) and rotate step (radians,
+ * double) per instance. Resets every slot to hold temperature index = slot. */
+int remc_set_replica_params(remc_handle* h, const float* ladder, const float* translate_step,
+                            const double* rotate_step);
+
+/* Full-system energy of every instance (kcal/mol), written to out[n_inst]
+ * (host) when out != NULL; also becomes each instance's running energy. */
+int remc_energy_full(remc_handle* h, double* out);
+int remc_get_energies(remc_handle* h, double* out);
+
+/* Advance every replica of every system by n_steps Metropolis steps (one
+ * persistent launch per sweep). Random numbers: Philox4x32-10 with key =
+ * seed, counter = (step0 + s, slot, system, purpose). */
+int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0);
+/* Same trajectory as remc_sweep, one kernel launch per replica per step
+ * (the per-replica launch pattern of the reference). */
+int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0);
+
+/* One exchange round in every system: temperature pairs (t, t+1) for
+ * t = offset, offset + 2, ...; counter = (round, pair, system, 2). */
+int remc_exchange(remc_handle* h, uint64_t seed, uint32_t round, int offset);
+
+/* temp_of_slot[n_inst]: temperature index held by each instance's slot. */
+int remc_get_temperature_map(remc_handle* h, int* temp_of_slot);
+/* Per-instance move counters since the last reset: accepted with dE < 0,
+ * accepted by the Boltzmann test, rejected; exchange counters per system. */
+int remc_get_counters(remc_handle* h, int* accept, int* acceptA, int* reject);
+int remc_reset_counters(remc_handle* h);
+
+/* Pair evaluations made by the sweeps since the last counter reset, summed
+ * over instances: residue-residue pairs (Kim-Hummer + Debye-Hueckel) and
+ * pairs involving a crowder. A dE pair counts twice (old and new position). */
+int remc_get_pair_evaluations(remc_handle* h, uint64_t* residue_pairs, uint64_t* crowder_pairs);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after the engine's. */
+int remc_get_stream(remc_handle* h, void** stream);
+
+/* dE of moving molecule `mol` of instance `inst` to new_pos (3 floats per
+ * bead, host), FP32 pairs with FP64 sum; the state is not changed. */
+int remc_delta_energy(remc_handle* h, int inst, int mol, const float* new_pos, double* dE);
+
+/* Run n_blocks of (sweep of steps_per_block steps, exchange round), the step
+ * and round counters advancing on the device, as one CUDA graph per block
+ * (captured on first use, replayed afterwards). */
+int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, uint32_t step0,
+             uint32_t round0);
+
+int remc_sync(remc_handle* h);
+int remc_num_instances(const remc_handle* h);
+const char* remc_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,108 @@
+"""Build recipe for the test oracles (TEST INFRASTRUCTURE).
+
+Produces:
+  oracle/_build/libremc_oracle.so  - the FP64 C restatement (remc_oracle.c)
+  oracle/_ref/libremcref.so        - the reference CPU engine's own sources
+                                     (compiled unmodified from the reference
+                                     tree) + ref_harness.cpp
+  oracle/_ref/REMCDockingCPU       - the reference CPU executable, same sources
+                                     + its main.cpp
+
+The reference tree is read where it lies (default
+/root/reference/simulation engine/src, override with REMC_REFERENCE_SRC);
+nothing is copied into this repository. Missing GSL / cutil headers are
+replaced by the project-written stubs in oracle/ref_stubs/. When the tree is
+absent (e.g. on a machine that only received the prebuilt files) the
+reference build is skipped and the prebuilt files are used as they are.
+
+Usage: python oracle/build.py [--force]
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+STUBS = os.path.join(HERE, "ref_stubs")
+DEFAULT_REF_SRC = "/root/reference/simulation engine/src"
+REF_UNITS = ["AminoAcid", "AminoAcids", "Link", "Molecule", "Quaternion", "Replica", "Residue",
+             "TorsionalLookupMatrix", "vector3f"]
+# the reference's own CPU flags (simulation engine/Makefile:17); gnu++11 only
+# because the stubs use <chrono>; -fpermissive for its pre-standard C++.
+REF_CFLAGS = ["-std=gnu++11", "-fpermissive", "-w", "-O2", "-fno-omit-frame-pointer", "-fPIC"]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+
+
+def _stale(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    src = os.path.join(HERE, "remc_oracle.c")
+    out = os.path.join(BUILD, "libremc_oracle.so")
+    if force or _stale(out, [src, os.path.join(HERE, "remc_oracle.h")]):
+        # default x86-64 target: no FMA, so FP32/FP64 ops round like the reference's
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-std=c99", "-o", out, src, "-lm"])
+    return out
+
+
+def reference_src() -> str:
+    return os.environ.get("REMC_REFERENCE_SRC", DEFAULT_REF_SRC)
+
+
+def build_reference(force: bool = False) -> bool:
+    """Compile the reference engine (unmodified) + harness. Returns False when
+    the reference tree is not present here."""
+    src_dir = reference_src()
+    if not os.path.isdir(src_dir):
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    objdir = os.path.join(REF_OUT, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I" + STUBS, "-I" + src_dir, "-I/usr/local/cuda/include"]
+    stub_files = [os.path.join(dp, f) for dp, _, fs in os.walk(STUBS) for f in fs]
+    objs = []
+    for unit in REF_UNITS + ["main"]:
+        s = os.path.join(src_dir, unit + ".cpp")
+        o = os.path.join(objdir, unit + ".o")
+        if force or _stale(o, [s] + stub_files):
+            _run(["g++"] + REF_CFLAGS + inc + ["-c", s, "-o", o])
+        objs.append(o)
+    harness_src = os.path.join(HERE, "ref_harness.cpp")
+    harness_obj = os.path.join(objdir, "ref_harness.o")
+    if force or _stale(harness_obj, [harness_src] + stub_files):
+        _run(["g++"] + REF_CFLAGS + inc + ["-c", harness_src, "-o", harness_obj])
+    lib = os.path.join(REF_OUT, "libremcref.so")
+    lib_objs = [o for o in objs if not o.endswith("main.o")] + [harness_obj]
+    if force or _stale(lib, lib_objs):
+        _run(["g++", "-shared", "-o", lib] + lib_objs + ["-lpthread"])
+    exe = os.path.join(REF_OUT, "REMCDockingCPU")
+    main_objs = [o for o in objs]
+    if force or _stale(exe, main_objs):
+        # -lcudart only for the one cudaGetErrorString call (main.cpp:1281)
+        _run(["g++", "-o", exe] + main_objs +
+             ["-lpthread", "-L/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64"])
+    return True
+
+
+def main() -> int:
+    force = "--force" in sys.argv
+    print("oracle:", build_oracle(force))
+    print("reference:", "built" if build_reference(force) else "tree absent, skipped")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

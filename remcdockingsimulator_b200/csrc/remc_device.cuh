@@ -1,0 +1,200 @@
+// Device building blocks of the B200 REMC engine: Philox stream, pair energy,
+// bead packing, exact-rounding move arithmetic.
+//
+// Pair energy: the Kim-Hummer-style contact term + Debye-Hueckel term of
+// Replica::E (simulation engine/src/Replica.cpp:603-745), with the crowder
+// branch of Replica.cpp:637-690 (mode 0) or an eps_c ((rho_i+rho_j)/r)^12 wall
+// (mode 1). Pair terms are FP32 with MUFU rsqrt/ex2; all per-type constants
+// (4 eps, sigma^2, the repulsive-branch threshold, q_i q_j and the unit
+// conversion factors) are folded into one float4 table entry per type pair.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/remc_b200.h"
+
+namespace remc {
+
+constexpr int kNT = REMC_MAX_TYPES;  // type-table edge
+constexpr int kNumAmino = REMC_NUM_AMINO;
+
+// ---------------------------------------------------------------- packing
+// A bead is one float4 in HBM and shared memory: x, y, z and, in .w, the bits
+// of (molecule index << 8 | type).
+__host__ __device__ __forceinline__ int pack_meta(int mol, int type) { return (mol << 8) | type; }
+__device__ __forceinline__ int bead_type(float w) { return __float_as_int(w) & 0xff; }
+__device__ __forceinline__ int bead_mol(float w) { return __float_as_int(w) >> 8; }
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon et al., SC'11): multipliers 0xD2511F53 / 0xCD9E8D57,
+// key increments 0x9E3779B9 / 0xBB67AE85, ten rounds.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k.x += 0x9E3779B9u;
+      k.y += 0xBB67AE85u;
+    }
+    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+  }
+  return c;
+}
+__device__ __forceinline__ double u32_unit(uint32_t x) {
+  return __dmul_rn((double)x, 2.3283064365386963e-10);  // 2^-32, exact
+}
+
+// ---------------------------------------------------------------- MUFU
+__device__ __forceinline__ float fast_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float fast_ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// ---------------------------------------------------------------- energy
+struct EnergyConsts {
+  float c_xi;        // -log2(e) / Xi: exp(-r/Xi) = ex2(r * c_xi)
+  int crowder_mode;  // 0: A r^-6; 1: A r^-12
+};
+
+// Minimum image d - L*rint(d/L) per axis (CudaFunctions.cu:430-442 uses rintf).
+__device__ __forceinline__ float min_image(float d, float L, float invL) {
+  return fmaf(-L, rintf(d * invL), d);
+}
+
+// Energy (kcal/mol) of one pair of beads of different molecules at squared
+// distance r2. T = table entry {4 eps', sigma^2, select threshold r^2, q q'}
+// for residue pairs, {A, 0, cutoff^2, 0} for crowder pairs.
+__device__ __forceinline__ float pair_energy_r2(float r2, float4 T, bool crowd,
+                                                const EnergyConsts& K) {
+  float rinv = fast_rsqrt(r2);
+  float rinv2 = rinv * rinv;
+  if (crowd) {
+    float i6 = rinv2 * rinv2 * rinv2;
+    float e = T.x * i6;
+    if (K.crowder_mode) e *= i6;
+    return (r2 < T.z) ? e : 0.0f;
+  }
+  float s2 = T.y * rinv2;
+  float s6 = s2 * s2 * s2;
+  float lj = T.x * fmaf(-s6, s6, s6);  // 4 eps' s6 (1 - s6) = -4 eps' s6 (s6 - 1)
+  lj = (r2 < T.z) ? fmaf(0.5f, T.x, -lj) : lj;  // repulsive branch: 2 eps' - LJ
+  float r = r2 * rinv;
+  float dh = T.w * fast_ex2(r * K.c_xi) * rinv;
+  return lj + dh;
+}
+
+__device__ __forceinline__ float pair_r2(float4 a, float4 b, float L, float invL) {
+  float dx = min_image(a.x - b.x, L, invL);
+  float dy = min_image(a.y - b.y, L, invL);
+  float dz = min_image(a.z - b.z, L, invL);
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// ---------------------------------------------------------------- moves
+// Exact-rounding (no FMA contraction) restatement of the reference's rigid-move
+// arithmetic so device trajectories round exactly like the host engine's:
+// Replica::createNormalisedRandomVector{,d} (Replica.cpp:303-318),
+// Replica::translate (:333-364), Molecule::rotateQ (Molecule.cpp:288-333),
+// Quaternion::rotateVector (Quaternion.cpp:84-101), Quaternion::multiply
+// (Quaternion.cpp:36-48).
+struct QuatProducts {
+  double a, b, c;  // row-0 terms: (w2+x2-y2-z2), (xy-wz), (wy+xz)
+  double d, e, f;  // row-1 terms: (wz+xy), (yz-wx), (w2-x2+y2-z2)
+  double g, h, i;  // row-2 terms: (xz-wy), (yz+wx), (w2-x2-y2+z2)
+};
+
+__device__ __forceinline__ QuatProducts quat_products(double w, double x, double y, double z) {
+  double w2 = __dmul_rn(w, w), x2 = __dmul_rn(x, x), y2 = __dmul_rn(y, y), z2 = __dmul_rn(z, z);
+  double wx = __dmul_rn(w, x), wy = __dmul_rn(w, y), wz = __dmul_rn(w, z);
+  double xy = __dmul_rn(x, y), xz = __dmul_rn(x, z), yz = __dmul_rn(y, z);
+  QuatProducts p;
+  p.a = __dsub_rn(__dsub_rn(__dadd_rn(w2, x2), y2), z2);
+  p.b = __dsub_rn(xy, wz);
+  p.c = __dadd_rn(wy, xz);
+  p.d = __dadd_rn(wz, xy);
+  p.e = __dsub_rn(yz, wx);
+  p.f = __dsub_rn(__dadd_rn(__dsub_rn(w2, x2), y2), z2);
+  p.g = __dsub_rn(xz, wy);
+  p.h = __dadd_rn(yz, wx);
+  p.i = __dadd_rn(__dsub_rn(__dsub_rn(w2, x2), y2), z2);
+  return p;
+}
+
+// rel' = q.rotateVector(rel), rounded to float as the reference's Vector3f
+// constructor does.
+__device__ __forceinline__ float3 rotate_rel(const QuatProducts& p, float rx, float ry, float rz) {
+  double vx = rx, vy = ry, vz = rz;
+  double X = __dadd_rn(__dmul_rn(vx, p.a),
+                       __dmul_rn(__dadd_rn(__dmul_rn(vy, p.b), __dmul_rn(vz, p.c)), 2.0));
+  double Y = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(vx, p.d), __dmul_rn(vz, p.e)), 2.0),
+                       __dmul_rn(vy, p.f));
+  double Z = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(vx, p.g), __dmul_rn(vy, p.h)), 2.0),
+                       __dmul_rn(vz, p.i));
+  return make_float3(__double2float_rn(X), __double2float_rn(Y), __double2float_rn(Z));
+}
+
+// q * r (Quaternion::multiply), exact rounding, left-to-right sums.
+__device__ __forceinline__ void quat_mul(double qw, double qx, double qy, double qz, double rw,
+                                         double rx, double ry, double rz, double out[4]) {
+  out[0] = __dsub_rn(__dsub_rn(__dsub_rn(__dmul_rn(qw, rw), __dmul_rn(qx, rx)), __dmul_rn(qy, ry)),
+                     __dmul_rn(qz, rz));
+  out[1] = __dsub_rn(__dadd_rn(__dadd_rn(__dmul_rn(qw, rx), __dmul_rn(qx, rw)), __dmul_rn(qy, rz)),
+                     __dmul_rn(qz, ry));
+  out[2] = __dadd_rn(__dadd_rn(__dsub_rn(__dmul_rn(qw, ry), __dmul_rn(qx, rz)), __dmul_rn(qy, rw)),
+                     __dmul_rn(qz, rx));
+  out[3] = __dadd_rn(__dsub_rn(__dadd_rn(__dmul_rn(qw, rz), __dmul_rn(qx, ry)), __dmul_rn(qy, rx)),
+                     __dmul_rn(qz, rw));
+}
+
+// Translation vector: translate_step * normalise(u2-.5, .5-u3, u4-.5) in FP32.
+__device__ __forceinline__ float3 translate_vector(double u2, double u3, double u4, float step) {
+  float vx = __double2float_rn(__dsub_rn(u2, 0.5));
+  float vy = __double2float_rn(__dsub_rn(0.5, u3));
+  float vz = __double2float_rn(__dsub_rn(u4, 0.5));
+  float mag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                   __fmul_rn(vz, vz)));
+  if (mag != 0.0f) {
+    vx = __fdiv_rn(vx, mag);
+    vy = __fdiv_rn(vy, mag);
+    vz = __fdiv_rn(vz, mag);
+  }
+  return make_float3(__fmul_rn(vx, step), __fmul_rn(vy, step), __fmul_rn(vz, step));
+}
+
+// Step quaternion for a rotation by a fixed angle about the random axis
+// normalise(u2-.5, .5-u3, u4-.5); cos/sin of the half angle come from the
+// host (they are per-replica constants).
+__device__ __forceinline__ void step_quaternion(double u2, double u3, double u4, double cosa,
+                                                double sina, double q[4]) {
+  double ax = __dsub_rn(u2, 0.5), ay = __dsub_rn(0.5, u3), az = __dsub_rn(u4, 0.5);
+  double am = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)),
+                                   __dmul_rn(az, az)));
+  ax = __ddiv_rn(ax, am);
+  ay = __ddiv_rn(ay, am);
+  az = __ddiv_rn(az, am);
+  double qw = cosa, qx = __dmul_rn(sina, ax), qy = __dmul_rn(sina, ay), qz = __dmul_rn(sina, az);
+  double qm = __dsqrt_rn(__dadd_rn(
+      __dadd_rn(__dadd_rn(__dmul_rn(qw, qw), __dmul_rn(qx, qx)), __dmul_rn(qy, qy)),
+      __dmul_rn(qz, qz)));
+  q[0] = __ddiv_rn(qw, qm);
+  q[1] = __ddiv_rn(qx, qm);
+  q[2] = __ddiv_rn(qy, qm);
+  q[3] = __ddiv_rn(qz, qm);
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  return v;
+}
+
+}  // namespace remc

@@ -1,0 +1,1270 @@
+// B200 replica-exchange Monte Carlo engine: kernels and the C ABI of
+// include/remc_b200.h.
+//
+// Data layout in HBM (all replica-instances of all systems of one handle):
+//   pos    float4[inst beads]  x, y, z, bits(mol << 8 | type)   (SoA per bead)
+//   rel    float4[inst beads]  position relative to the molecule centre
+//   centre float4[inst mols]   molecule centre (Molecule::center)
+//   quat   double[4*inst mols] accumulated rotation (Molecule::rotation)
+//   energy double[inst]        running total energy (Replica::potential)
+// Instance g of system s, slot k: beads at bead_base(s) + k*N_s, molecules at
+// mol_base(s) + k*M_s.
+//
+// Kernels:
+//   sweep_kernel       one CTA per replica-instance, persistent over a whole
+//                      sweep of n_steps Metropolis steps; the instance's beads
+//                      and molecule centres stay resident in shared memory, each
+//                      step is proposal -> trial positions -> FP32 pair dE with
+//                      FP64 reduction -> Metropolis (Replica::MCSearch,
+//                      Replica.cpp:368-478, with dE in place of the full E).
+//   energy_tile_kernel persistent grid over (instance, i-tile, j-tile) work
+//                      items of the upper triangle; per-item FP64 partials in a
+//                      scratch array, reduced per instance in fixed order by
+//                      energy_reduce_kernel (Replica::E / E_TiledKernel,
+//                      CudaFunctions.cu:455-685).
+//   exchange_kernel    one warp per system, disjoint temperature pairs in
+//                      parallel lanes (main.cpp:1427-1453).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "remc_device.cuh"
+
+using namespace remc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define REMC_CUDA_TRY(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return set_error(REMC_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(_e));   \
+  } while (0)
+
+struct SysDev {
+  int n_beads, n_mol, n_rep, lmax;
+  int inst0, bead_base, mol_base, mstart_off;
+  float box, invbox;
+  int translate_only_crowders;
+  int n_chain_beads;  // beads of residue type; the rest are crowders
+};
+
+// Per-step proposal data computed 32 steps at a time by warp 0.
+struct StepInfo {
+  double q[4];      // step quaternion (rotation)
+  double u5;        // Metropolis uniform
+  float t[3];       // translation vector
+  int m;            // molecule
+  int rotate;       // 1 rotation, 0 translation
+  int pad;
+};
+static_assert(sizeof(StepInfo) == 64, "StepInfo layout");
+
+struct SweepArgs {
+  const SysDev* sys;
+  const int* inst_sys;
+  const int* inst_list;  // CTA -> instance
+  float4* pos;
+  float4* rel;
+  float4* centre;
+  double* quat;
+  const int* mol_start;
+  const float4* tab;
+  double* energy;
+  const int* temp_idx;
+  const float* ladder;
+  const float* tstep;
+  const double* rot_cs;  // cos, sin of the half rotate step per instance
+  int* acc_neg;          // accepted with dE < 0
+  int* acc_boltz;        // accepted by the Boltzmann test
+  int* rej;
+  unsigned long long* evals_kh;     // residue-residue pair evaluations
+  unsigned long long* evals_crowd;  // pair evaluations involving a crowder
+  const uint32_t* ctrl;  // device step counter (graph mode) or null
+  uint32_t step0;
+  uint32_t seed_lo, seed_hi;
+  int n_steps;
+  int nmax, mmax, lmax;  // shared-memory capacities
+  EnergyConsts K;
+};
+
+// Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
+// mmax molecules, lmax beads per molecule, nwarps).
+struct SweepSmem {
+  size_t tab, beads, centres, trial_pos, trial_rel, mstart, info, red, total;
+  static __host__ __device__ size_t take(size_t& off, size_t bytes) {
+    size_t o = off;
+    off += (bytes + 15) & ~size_t(15);
+    return o;
+  }
+  static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax) {
+    SweepSmem s;
+    size_t off = 0;
+    s.tab = take(off, sizeof(float4) * kNT * kNT);
+    s.beads = take(off, sizeof(float4) * nmax);
+    s.centres = take(off, sizeof(float4) * mmax);
+    s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
+    s.trial_rel = take(off, sizeof(float4) * 2 * lmax);
+    s.mstart = take(off, sizeof(int) * (mmax + 1));
+    s.info = take(off, sizeof(StepInfo) * 32);
+    s.red = take(off, sizeof(double) * 32 + 64);
+    s.total = off;
+    return s;
+  }
+};
+
+// Control block written by thread 0 each step, read by all after a barrier.
+struct StepCtl {
+  float nc[3];
+  int m0, n_m, rotate, skip, buf;
+  // previous step (applied at the start of this step)
+  int p_acc, p_m0, p_n, p_rot, p_buf;
+};
+
+__global__ void __launch_bounds__(512) sweep_kernel(SweepArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax);
+  float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
+  float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
+  float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
+  float4* s_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
+  float4* s_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
+  int* s_mstart = reinterpret_cast<int*>(smem_raw + L.mstart);
+  StepInfo* s_info = reinterpret_cast<StepInfo*>(smem_raw + L.info);
+  double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
+  __shared__ StepCtl ctl;
+
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+  const int inst = A.inst_list[blockIdx.x];
+  const int sysid = A.inst_sys[inst];
+  const SysDev S = A.sys[sysid];
+  const int slot = inst - S.inst0;
+  const int N = S.n_beads, M = S.n_mol;
+  const int bead_off = S.bead_base + slot * N;
+  const int mol_off = S.mol_base + slot * M;
+  const float box = S.box, invbox = S.invbox;
+  const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
+
+  // ---- prologue: make the instance resident in shared memory
+  for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
+  for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
+  for (int i = tid; i < M; i += nthr) s_cent[i] = A.centre[mol_off + i];
+  for (int i = tid; i <= M; i += nthr) s_mstart[i] = A.mol_start[S.mstart_off + i];
+
+  const float T = A.ladder[S.inst0 + A.temp_idx[inst]];
+  const float tstep = A.tstep[inst];
+  const double cosa = A.rot_cs[2 * inst], sina = A.rot_cs[2 * inst + 1];
+  double energy = 0.0;
+  int n_neg = 0, n_boltz = 0, n_rej = 0;
+  unsigned long long ev_kh = 0, ev_crowd = 0;
+  if (tid == 0) {
+    energy = A.energy[inst];
+    ctl.p_acc = 0;
+  }
+  const double beta = 4184.0 / ((double)8.314472f * (double)T);
+  __syncthreads();
+
+  for (int s = 0; s < A.n_steps; ++s) {
+    // ---- warp 0: proposals for the next 32 steps (Philox + normalisations)
+    if (warp == 0) {
+      if ((s & 31) == 0) {
+        int st = s + lane;
+        if (st < A.n_steps) {
+          uint4 c = make_uint4(step0 + (uint32_t)st, (uint32_t)slot, (uint32_t)sysid, 0u);
+          uint2 k = make_uint2(A.seed_lo, A.seed_hi);
+          uint4 x = philox4x32_10(c, k);
+          c.w = 1u;
+          uint4 y = philox4x32_10(c, k);
+          double u0 = u32_unit(x.x), u1 = u32_unit(x.y), u2 = u32_unit(x.z), u3 = u32_unit(x.w);
+          double u4 = u32_unit(y.x), u5 = u32_unit(y.y);
+          StepInfo inf;
+          inf.m = (int)__dmul_rn(u0, (double)M);
+          int crowd = bead_type(s_beads[s_mstart[inf.m]].w) >= kNumAmino;
+          inf.rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
+          inf.u5 = u5;
+          if (inf.rotate) {
+            step_quaternion(u2, u3, u4, cosa, sina, inf.q);
+            inf.t[0] = inf.t[1] = inf.t[2] = 0.0f;
+          } else {
+            float3 t = translate_vector(u2, u3, u4, tstep);
+            inf.t[0] = t.x;
+            inf.t[1] = t.y;
+            inf.t[2] = t.z;
+            inf.q[0] = 1.0;
+            inf.q[1] = inf.q[2] = inf.q[3] = 0.0;
+          }
+          inf.pad = 0;
+          s_info[lane] = inf;
+        }
+        __syncwarp();
+      }
+      if (lane == 0) {
+        const StepInfo& inf = s_info[s & 31];
+        int m = inf.m;
+        int m0 = s_mstart[m], n = s_mstart[m + 1] - m0;
+        float4 c = s_cent[m];
+        float nc0 = c.x, nc1 = c.y, nc2 = c.z;
+        if (!inf.rotate) {
+          nc0 = fmodf(__fadd_rn(__fadd_rn(c.x, inf.t[0]), box), box);
+          nc1 = fmodf(__fadd_rn(__fadd_rn(c.y, inf.t[1]), box), box);
+          nc2 = fmodf(__fadd_rn(__fadd_rn(c.z, inf.t[2]), box), box);
+        }
+        ctl.nc[0] = nc0;
+        ctl.nc[1] = nc1;
+        ctl.nc[2] = nc2;
+        ctl.m0 = m0;
+        ctl.n_m = n;
+        ctl.rotate = inf.rotate;
+        ctl.skip = inf.rotate && n == 1;  // a one-bead rotation moves nothing: dE = 0
+        ctl.buf = s & 1;
+      }
+    }
+    __syncthreads();  // A: proposal ready, previous decision visible
+
+    // ---- apply the previous accepted move, build this step's trial positions
+    {
+      const int m0 = ctl.m0, n = ctl.n_m, rot = ctl.rotate, b = ctl.buf;
+      const int pacc = ctl.p_acc, pm0 = ctl.p_m0, pn = ctl.p_n, prot = ctl.p_rot, pb = ctl.p_buf;
+      if (pacc) {
+        for (int k = tid; k < pn; k += nthr) {
+          s_beads[pm0 + k] = s_tpos[pb * A.lmax + k];
+          if (prot && pn > 1) A.rel[bead_off + pm0 + k] = s_trel[pb * A.lmax + k];
+        }
+      }
+      const float nc0 = ctl.nc[0], nc1 = ctl.nc[1], nc2 = ctl.nc[2];
+      if (rot) {
+        if (n > 1) {
+          const StepInfo& inf = s_info[s & 31];
+          QuatProducts qp = quat_products(inf.q[0], inf.q[1], inf.q[2], inf.q[3]);
+          for (int k = tid; k < n; k += nthr) {
+            float4 rl = A.rel[bead_off + m0 + k];
+            float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
+            float w = s_beads[m0 + k].w;
+            s_trel[b * A.lmax + k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
+            s_tpos[b * A.lmax + k] =
+                make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
+          }
+        } else if (tid == 0) {
+          s_tpos[b * A.lmax] = s_beads[m0];
+        }
+      } else {
+        for (int k = tid; k < n; k += nthr) {
+          float4 rl = (n > 1) ? A.rel[bead_off + m0 + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+          float w = s_beads[m0 + k].w;
+          s_tpos[b * A.lmax + k] =
+              make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
+        }
+      }
+    }
+    __syncthreads();  // T: beads current, trial ready
+
+    // ---- dE = sum over beads k of the molecule, beads j outside it
+    double dacc = 0.0;
+    if (!ctl.skip) {
+      const int m0 = ctl.m0, n = ctl.n_m, b = ctl.buf;
+      const int nrest = N - n;
+      for (int k = 0; k < n; ++k) {
+        const float4 pold = s_beads[m0 + k];
+        const float4 pnew = s_tpos[b * A.lmax + k];
+        const int ta = bead_type(pold.w);
+        const bool a_crowd = ta >= kNumAmino;
+        const float4* trow = s_tab + ta * kNT;
+        float acc = 0.0f;
+        for (int jj = tid; jj < nrest; jj += nthr) {
+          const int j = jj < m0 ? jj : jj + n;
+          const float4 pj = s_beads[j];
+          const int tb = bead_type(pj.w);
+          const float4 Tj = trow[tb];
+          const bool crowd = a_crowd || tb >= kNumAmino;
+          float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
+          float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
+          acc += en - eo;
+        }
+        dacc += (double)acc;
+      }
+    }
+    dacc = warp_sum(dacc);
+    if (lane == 0) s_red[warp] = dacc;
+    __syncthreads();  // R: partial sums ready
+
+    // ---- warp 0: reduce, Metropolis, bookkeeping
+    if (warp == 0) {
+      double v = lane < nwarps ? s_red[lane] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0) {
+        const StepInfo& inf = s_info[s & 31];
+        const double dE = v;
+        if (!ctl.skip) {
+          // two evaluations (old and new position) per pair
+          const unsigned long long n = (unsigned long long)ctl.n_m;
+          if (bead_type(s_beads[ctl.m0].w) >= kNumAmino) {
+            ev_crowd += 2ull * n * (unsigned long long)(N - ctl.n_m);
+          } else {
+            ev_kh += 2ull * n * (unsigned long long)(S.n_chain_beads - ctl.n_m);
+            ev_crowd += 2ull * n * (unsigned long long)(N - S.n_chain_beads);
+          }
+        }
+        int acc = 0;
+        if (dE < 0.0) {
+          acc = 1;
+        } else if (inf.u5 < exp(-dE * beta)) {
+          acc = 2;
+        }
+        if (acc) {
+          energy += dE;
+          if (acc == 1) ++n_neg; else ++n_boltz;
+          const int m = inf.m;
+          if (inf.rotate) {
+            double* qd = A.quat + 4 * (size_t)(mol_off + m);
+            double out[4];
+            quat_mul(inf.q[0], inf.q[1], inf.q[2], inf.q[3], qd[0], qd[1], qd[2], qd[3], out);
+            qd[0] = out[0];
+            qd[1] = out[1];
+            qd[2] = out[2];
+            qd[3] = out[3];
+          } else {
+            float4 c = s_cent[m];
+            s_cent[m] = make_float4(ctl.nc[0], ctl.nc[1], ctl.nc[2], c.w);
+          }
+        } else {
+          ++n_rej;
+        }
+        ctl.p_acc = acc != 0;
+        ctl.p_m0 = ctl.m0;
+        ctl.p_n = ctl.n_m;
+        ctl.p_rot = ctl.rotate;
+        ctl.p_buf = ctl.buf;
+      }
+    }
+    // the next iteration's barrier A orders these writes before their use
+  }
+  __syncthreads();
+
+  // ---- epilogue: apply the last accepted move, write the instance back
+  {
+    const int pacc = ctl.p_acc, pm0 = ctl.p_m0, pn = ctl.p_n, prot = ctl.p_rot, pb = ctl.p_buf;
+    if (pacc && A.n_steps > 0) {
+      for (int k = tid; k < pn; k += nthr) {
+        s_beads[pm0 + k] = s_tpos[pb * A.lmax + k];
+        if (prot && pn > 1) A.rel[bead_off + pm0 + k] = s_trel[pb * A.lmax + k];
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
+  for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
+  if (tid == 0) {
+    A.energy[inst] = energy;
+    A.acc_neg[inst] += n_neg;
+    A.acc_boltz[inst] += n_boltz;
+    A.rej[inst] += n_rej;
+    A.evals_kh[inst] += ev_kh;
+    A.evals_crowd[inst] += ev_crowd;
+  }
+}
+
+// ------------------------------------------------------------------ full E
+struct TileItem {
+  int inst, ti, tj, pad;
+};
+
+constexpr int kTile = 128;
+
+__global__ void __launch_bounds__(kTile) energy_tile_kernel(
+    const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
+    const float4* __restrict__ pos, const float4* __restrict__ tab,
+    const TileItem* __restrict__ items, int n_items, double* __restrict__ scratch,
+    EnergyConsts K) {
+  __shared__ float4 s_tab[kNT * kNT];
+  __shared__ float4 s_j[kTile];
+  __shared__ double s_red[kTile / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const TileItem W = items[it];
+    const SysDev S = sys[inst_sys[W.inst]];
+    const int N = S.n_beads;
+    const int base = S.bead_base + (W.inst - S.inst0) * N;
+    const float box = S.box, invbox = S.invbox;
+    const int j0 = W.tj * kTile;
+    const int jn = min(kTile, N - j0);
+    __syncthreads();  // previous item done with s_j
+    if (tid < jn) s_j[tid] = pos[base + j0 + tid];
+    __syncthreads();
+    const int i = W.ti * kTile + tid;
+    double dsum = 0.0;
+    if (i < N) {
+      const float4 pi = pos[base + i];
+      const int ta = bead_type(pi.w), mi = bead_mol(pi.w);
+      const bool a_crowd = ta >= kNumAmino;
+      const int jstart = (W.ti == W.tj) ? tid + 1 : 0;
+      float acc = 0.0f;
+      for (int jj = jstart; jj < jn; ++jj) {
+        const float4 pj = s_j[jj];
+        if (bead_mol(pj.w) == mi) continue;
+        const int tb = bead_type(pj.w);
+        const float4 Tij = s_tab[tb * kNT + ta];
+        acc += pair_energy_r2(pair_r2(pi, pj, box, invbox), Tij, a_crowd || tb >= kNumAmino, K);
+      }
+      dsum = (double)acc;
+    }
+    dsum = warp_sum(dsum);
+    if (lane == 0) s_red[warp] = dsum;
+    __syncthreads();
+    if (tid == 0) {
+      double v = 0.0;
+      for (int w = 0; w < kTile / 32; ++w) v += s_red[w];
+      scratch[it] = v;
+    }
+  }
+}
+
+// Per-instance fixed-order sum of the tile partials.
+__global__ void energy_reduce_kernel(const int* __restrict__ item_off, int n_inst,
+                                     const double* __restrict__ scratch, double* __restrict__ energy) {
+  const int inst = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (inst >= n_inst) return;
+  const int a = item_off[inst], b = item_off[inst + 1];
+  double v = 0.0;
+  for (int i = a + lane; i < b; i += 32) v += scratch[i];
+  v = warp_sum(v);
+  if (lane == 0) energy[inst] = v;
+}
+
+// ------------------------------------------------------------------ exchange
+__global__ void exchange_kernel(const SysDev* __restrict__ sys, const float* __restrict__ ladder,
+                                const double* __restrict__ energy, int* __restrict__ temp_idx,
+                                int* __restrict__ slot_of_temp, int* __restrict__ ex_tests,
+                                int* __restrict__ ex_acc, const uint32_t* ctrl, uint32_t round_arg,
+                                int offset_arg, uint32_t seed_lo, uint32_t seed_hi) {
+  const int sysid = blockIdx.x;
+  const SysDev S = sys[sysid];
+  const int R = S.n_rep;
+  const uint32_t round = ctrl ? ctrl[1] : round_arg;
+  const int offset = ctrl ? (int)(ctrl[2] & 1u) : offset_arg;
+  int tests = 0, accs = 0;
+  for (int p = threadIdx.x; offset + 2 * p < R - 1; p += blockDim.x) {
+    const int t = offset + 2 * p;
+    const int a = slot_of_temp[S.inst0 + t], b = slot_of_temp[S.inst0 + t + 1];
+    const double Ti = (double)ladder[S.inst0 + t], Tj = (double)ladder[S.inst0 + t + 1];
+    const double delta = (1.0 / Ti - 1.0 / Tj) * (energy[S.inst0 + a] - energy[S.inst0 + b]) *
+                         (double)(4184.0f / 8.314472f);
+    uint4 x = philox4x32_10(make_uint4(round, (uint32_t)p, (uint32_t)sysid, 2u),
+                            make_uint2(seed_lo, seed_hi));
+    const double u = u32_unit(x.x);
+    double pacc = exp(delta);
+    if (pacc > 1.0) pacc = 1.0;
+    ++tests;
+    if (u < pacc) {
+      ++accs;
+      slot_of_temp[S.inst0 + t] = b;
+      slot_of_temp[S.inst0 + t + 1] = a;
+      temp_idx[S.inst0 + a] = t + 1;
+      temp_idx[S.inst0 + b] = t;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    tests += __shfl_down_sync(0xffffffffu, tests, off);
+    accs += __shfl_down_sync(0xffffffffu, accs, off);
+  }
+  if (threadIdx.x == 0) {
+    ex_tests[sysid] += tests;
+    ex_acc[sysid] += accs;
+  }
+}
+
+// Advance the device step/round/offset counters between graph replays.
+__global__ void ctrl_advance_kernel(uint32_t* ctrl, uint32_t steps) {
+  ctrl[0] += steps;
+  ctrl[1] += 1u;
+  ctrl[2] ^= 1u;
+}
+
+// ------------------------------------------------------------------ dE API
+__global__ void delta_kernel(const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
+                             const float4* __restrict__ pos, const float4* __restrict__ tab,
+                             const int* __restrict__ mol_start, int inst, int mol,
+                             const float4* __restrict__ newpos, double* __restrict__ out,
+                             EnergyConsts K) {
+  __shared__ double s_red[32];
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const SysDev S = sys[inst_sys[inst]];
+  const int N = S.n_beads;
+  const int base = S.bead_base + (inst - S.inst0) * N;
+  const int m0 = mol_start[S.mstart_off + mol], n = mol_start[S.mstart_off + mol + 1] - m0;
+  double dacc = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const float4 pold = pos[base + m0 + k];
+    float4 pnew = newpos[k];
+    const int ta = bead_type(pold.w);
+    float acc = 0.0f;
+    for (int jj = tid; jj < N - n; jj += nthr) {
+      const int j = jj < m0 ? jj : jj + n;
+      const float4 pj = pos[base + j];
+      const int tb = bead_type(pj.w);
+      const float4 T = tab[ta * kNT + tb];
+      const bool crowd = ta >= kNumAmino || tb >= kNumAmino;
+      acc += pair_energy_r2(pair_r2(pnew, pj, S.box, S.invbox), T, crowd, K) -
+             pair_energy_r2(pair_r2(pold, pj, S.box, S.invbox), T, crowd, K);
+    }
+    dacc += (double)acc;
+  }
+  dacc = warp_sum(dacc);
+  if (lane == 0) s_red[warp] = dacc;
+  __syncthreads();
+  if (tid == 0) {
+    double v = 0.0;
+    for (int w = 0; w < nthr / 32; ++w) v += s_red[w];
+    *out = v;
+  }
+}
+
+}  // namespace
+
+// =================================================================== host
+struct remc_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  remc_params params{};
+  int n_sys = 0, n_inst = 0;
+  std::vector<SysDev> h_sys;
+  std::vector<int> h_inst_sys;
+  std::vector<int> h_mol_start;  // concatenated per system
+  std::vector<int> h_mol_role;
+  std::vector<int> h_bead_type;  // concatenated per system
+  std::vector<int> h_bead_off_static;
+  size_t total_beads = 0, total_mols = 0;
+  int nmax = 0, mmax = 0, lmax = 0;
+  // tables
+  float vdw[kNT] = {}, charge[kNT] = {}, rho[kNT] = {};
+  float pair_table[400] = {};
+  bool tables_set = false, state_set = false, replica_params_set = false;
+  // device
+  SysDev* d_sys = nullptr;
+  int* d_inst_sys = nullptr;
+  int* d_inst_list = nullptr;
+  float4* d_pos = nullptr;
+  float4* d_rel = nullptr;
+  float4* d_centre = nullptr;
+  double* d_quat = nullptr;
+  int* d_mol_start = nullptr;
+  float4* d_tab = nullptr;
+  double* d_energy = nullptr;
+  int* d_temp_idx = nullptr;
+  int* d_slot_of_temp = nullptr;
+  float* d_ladder = nullptr;
+  float* d_tstep = nullptr;
+  double* d_rot_cs = nullptr;
+  int* d_acc_neg = nullptr;
+  int* d_acc_boltz = nullptr;
+  int* d_rej = nullptr;
+  unsigned long long* d_evals_kh = nullptr;
+  unsigned long long* d_evals_crowd = nullptr;
+  int* d_ex_tests = nullptr;
+  int* d_ex_acc = nullptr;
+  uint32_t* d_ctrl = nullptr;
+  TileItem* d_items = nullptr;
+  int* d_item_off = nullptr;
+  double* d_scratch = nullptr;
+  int n_items = 0;
+  float4* d_newpos = nullptr;
+  double* d_dE = nullptr;
+  int sweep_threads = 128;
+  int num_sms = 148;
+  // graph
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_steps = -1;
+  uint64_t graph_seed = 0;
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess)
+    return set_error(REMC_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", n * sizeof(T),
+                     cudaGetErrorString(e));
+  return REMC_OK;
+}
+
+void free_all(remc_handle* h) {
+  void* ptrs[] = {h->d_sys,      h->d_inst_sys,  h->d_inst_list,  h->d_pos,        h->d_rel,
+                  h->d_centre,   h->d_quat,      h->d_mol_start,  h->d_tab,        h->d_energy,
+                  h->d_temp_idx, h->d_slot_of_temp, h->d_ladder,  h->d_tstep,      h->d_rot_cs,
+                  h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
+                  h->d_evals_kh, h->d_evals_crowd,
+                  h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
+                  h->d_dE};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+int build_tables(remc_handle* h) {
+  const remc_params& P = h->params;
+  std::vector<float4> tab(kNT * kNT);
+  const float c_lj = (float)((double)P.lj_cf * (double)P.kbt_cf);
+  const float c_dh = (float)((double)P.dh_const * (double)P.kbt_cf);
+  const float two_third = 1.2599210498948732f;  // 2^(1/3): (2^(1/6) sigma)^2 = 2^(1/3) sigma^2
+  for (int a = 0; a < kNT; ++a) {
+    for (int b = 0; b < kNT; ++b) {
+      float4 t;
+      if (a < kNumAmino && b < kNumAmino) {
+        // eps = lambda (M - e0) in FP32, as the reference evaluates it
+        float eps = P.lambda_ * (h->pair_table[a * 20 + b] - P.e0);
+        float epsc = eps * c_lj;
+        float sig = 0.5f * (h->vdw[a] + h->vdw[b]);
+        t.x = 4.0f * epsc;
+        t.y = sig * sig;
+        t.z = eps > 0.0f ? sig * sig * two_third : -1.0f;
+        t.w = h->charge[a] * h->charge[b] * c_dh;
+      } else {
+        double A;
+        if (P.crowder_mode == 0) {
+          A = 46656.0 * (double)c_lj;  // (6/r)^6 = 46656 r^-6
+        } else {
+          double sg = (double)h->rho[a] + (double)h->rho[b];
+          double s2 = sg * sg, s6 = s2 * s2 * s2;
+          A = (double)P.crowder_eps * s6 * s6 * (double)c_lj;
+        }
+        t.x = (float)A;
+        t.y = 0.0f;
+        t.z = P.crowder_cutoff > 0.0f ? P.crowder_cutoff * P.crowder_cutoff : INFINITY;
+        t.w = 0.0f;
+      }
+      tab[a * kNT + b] = t;
+    }
+  }
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_tab, tab.data(), sizeof(float4) * tab.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+EnergyConsts consts_of(const remc_handle* h) {
+  EnergyConsts K;
+  K.c_xi = (float)(-1.4426950408889634 / (double)h->params.debye_length);
+  K.crowder_mode = h->params.crowder_mode;
+  return K;
+}
+
+int check_ready(const remc_handle* h) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (!h->tables_set) return set_error(REMC_ERR_STATE, "type tables not set");
+  if (!h->state_set) return set_error(REMC_ERR_STATE, "state not uploaded");
+  if (!h->replica_params_set) return set_error(REMC_ERR_STATE, "replica parameters not set");
+  return REMC_OK;
+}
+
+int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0, const uint32_t* ctrl,
+                 const int* inst_list, int n_blocks) {
+  SweepArgs A;
+  A.sys = h->d_sys;
+  A.inst_sys = h->d_inst_sys;
+  A.inst_list = inst_list;
+  A.pos = h->d_pos;
+  A.rel = h->d_rel;
+  A.centre = h->d_centre;
+  A.quat = h->d_quat;
+  A.mol_start = h->d_mol_start;
+  A.tab = h->d_tab;
+  A.energy = h->d_energy;
+  A.temp_idx = h->d_temp_idx;
+  A.ladder = h->d_ladder;
+  A.tstep = h->d_tstep;
+  A.rot_cs = h->d_rot_cs;
+  A.acc_neg = h->d_acc_neg;
+  A.acc_boltz = h->d_acc_boltz;
+  A.rej = h->d_rej;
+  A.evals_kh = h->d_evals_kh;
+  A.evals_crowd = h->d_evals_crowd;
+  A.ctrl = ctrl;
+  A.step0 = step0;
+  A.seed_lo = (uint32_t)seed;
+  A.seed_hi = (uint32_t)(seed >> 32);
+  A.n_steps = n_steps;
+  A.nmax = h->nmax;
+  A.mmax = h->mmax;
+  A.lmax = h->lmax;
+  A.K = consts_of(h);
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax).total;
+  sweep_kernel<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
+  REMC_CUDA_TRY(cudaGetLastError());
+  return REMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void remc_default_params(remc_params* p) {
+  if (!p) return;
+  p->lambda_ = 0.159f;
+  p->e0 = -2.27f;
+  p->debye_length = 10.0f;
+  p->dh_const = 0.948f * 1.602176487f * 1.602176487f;  // Replica.cpp:624 (float arithmetic)
+  p->lj_cf = 0.3507221006079f;
+  p->kbt_cf = 1.0f / (294.0f * 8.314472f / 4184.0f);
+  p->crowder_mode = 0;
+  p->crowder_cutoff = 15.0f;
+  p->crowder_eps = 1.0f;
+}
+
+const char* remc_last_error_string(void) { return g_last_error.c_str(); }
+
+int remc_create(const remc_system_desc* systems, int n_systems, const remc_params* params,
+                remc_handle** out) {
+  if (!out) return set_error(REMC_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (!systems || n_systems <= 0) return set_error(REMC_ERR_INVALID, "no systems");
+  remc_handle* h = new (std::nothrow) remc_handle();
+  if (!h) return set_error(REMC_ERR_NOMEM, "host allocation failed");
+  if (params)
+    h->params = *params;
+  else
+    remc_default_params(&h->params);
+  // ---- validate and lay out
+  size_t bead_cursor = 0, mol_cursor = 0;
+  int inst_cursor = 0, mstart_cursor = 0;
+  for (int s = 0; s < n_systems; ++s) {
+    const remc_system_desc& d = systems[s];
+    if (d.n_beads <= 0 || d.n_mol <= 0 || d.n_replicas <= 0 || !d.mol_start || !d.mol_role ||
+        !d.bead_type || !(d.box > 0.0f) || !std::isfinite(d.box)) {
+      delete h;
+      return set_error(REMC_ERR_INVALID, "system %d: bad descriptor", s);
+    }
+    if (d.n_mol >= (1 << 22)) {
+      delete h;
+      return set_error(REMC_ERR_INVALID, "system %d: too many molecules", s);
+    }
+    if (d.mol_start[0] != 0 || d.mol_start[d.n_mol] != d.n_beads) {
+      delete h;
+      return set_error(REMC_ERR_INVALID, "system %d: mol_start must run 0..n_beads", s);
+    }
+    int lmax = 0;
+    for (int m = 0; m < d.n_mol; ++m) {
+      int n = d.mol_start[m + 1] - d.mol_start[m];
+      if (n <= 0) {
+        delete h;
+        return set_error(REMC_ERR_INVALID, "system %d: molecule %d is empty", s, m);
+      }
+      if (d.mol_role[m] != 0 && d.mol_role[m] != -1) {
+        delete h;
+        return set_error(REMC_ERR_INVALID, "system %d: molecule %d role must be 0 or -1", s, m);
+      }
+      for (int b = d.mol_start[m]; b < d.mol_start[m + 1]; ++b) {
+        int t = d.bead_type[b];
+        bool crowd_t = t >= kNumAmino;
+        if (t < 0 || t >= kNT || crowd_t != (d.mol_role[m] == -1)) {
+          delete h;
+          return set_error(REMC_ERR_INVALID,
+                           "system %d: bead %d type %d does not match molecule role", s, b, t);
+        }
+      }
+      lmax = std::max(lmax, n);
+    }
+    SysDev S{};
+    S.n_beads = d.n_beads;
+    S.n_mol = d.n_mol;
+    S.n_rep = d.n_replicas;
+    S.lmax = lmax;
+    S.inst0 = inst_cursor;
+    S.bead_base = (int)bead_cursor;
+    S.mol_base = (int)mol_cursor;
+    S.mstart_off = mstart_cursor;
+    S.box = d.box;
+    S.invbox = 1.0f / d.box;
+    S.translate_only_crowders = d.translate_only_crowders ? 1 : 0;
+    S.n_chain_beads = 0;
+    for (int b = 0; b < d.n_beads; ++b) S.n_chain_beads += d.bead_type[b] < kNumAmino ? 1 : 0;
+    h->h_sys.push_back(S);
+    for (int k = 0; k < d.n_replicas; ++k) h->h_inst_sys.push_back(s);
+    h->h_mol_start.insert(h->h_mol_start.end(), d.mol_start, d.mol_start + d.n_mol + 1);
+    h->h_mol_role.insert(h->h_mol_role.end(), d.mol_role, d.mol_role + d.n_mol);
+    h->h_bead_off_static.push_back((int)h->h_bead_type.size());
+    h->h_bead_type.insert(h->h_bead_type.end(), d.bead_type, d.bead_type + d.n_beads);
+    bead_cursor += (size_t)d.n_beads * d.n_replicas;
+    mol_cursor += (size_t)d.n_mol * d.n_replicas;
+    inst_cursor += d.n_replicas;
+    mstart_cursor += d.n_mol + 1;
+    h->nmax = std::max(h->nmax, d.n_beads);
+    h->mmax = std::max(h->mmax, d.n_mol);
+    h->lmax = std::max(h->lmax, lmax);
+  }
+  if (bead_cursor >= (size_t)1 << 31) {
+    delete h;
+    return set_error(REMC_ERR_INVALID, "too many beads in one handle");
+  }
+  h->n_sys = n_systems;
+  h->n_inst = inst_cursor;
+  h->total_beads = bead_cursor;
+  h->total_mols = mol_cursor;
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax).total;
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e != cudaSuccess) {
+    delete h;
+    return set_error(REMC_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  }
+  int max_smem = 0;
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+  if (smem > (size_t)max_smem) {
+    delete h;
+    return set_error(REMC_ERR_INVALID,
+                     "largest system needs %zu bytes of shared memory, device allows %d", smem,
+                     max_smem);
+  }
+  e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e != cudaSuccess) {
+    delete h;
+    return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+  }
+  // larger systems get more threads per replica
+  h->sweep_threads = h->nmax <= 1024 ? 128 : (h->nmax <= 4096 ? 256 : 512);
+  // ---- work list of the full-energy kernel (upper-triangle tiles)
+  std::vector<TileItem> items;
+  std::vector<int> item_off;
+  for (int g = 0; g < h->n_inst; ++g) {
+    item_off.push_back((int)items.size());
+    const SysDev& S = h->h_sys[h->h_inst_sys[g]];
+    int nt = (S.n_beads + kTile - 1) / kTile;
+    for (int ti = 0; ti < nt; ++ti)
+      for (int tj = ti; tj < nt; ++tj) items.push_back(TileItem{g, ti, tj, 0});
+  }
+  item_off.push_back((int)items.size());
+  h->n_items = (int)items.size();
+  // ---- device memory
+  int rc = REMC_OK;
+  e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) rc = set_error(REMC_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  std::vector<int> inst_list(h->n_inst);
+  for (int g = 0; g < h->n_inst; ++g) inst_list[g] = g;
+  // largest systems first: the block scheduler starts them earliest
+  std::stable_sort(inst_list.begin(), inst_list.end(), [&](int a, int b) {
+    return h->h_sys[h->h_inst_sys[a]].n_beads > h->h_sys[h->h_inst_sys[b]].n_beads;
+  });
+  if (!rc) rc = dev_alloc(&h->d_sys, h->h_sys.size());
+  if (!rc) rc = dev_alloc(&h->d_inst_sys, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_inst_list, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_pos, h->total_beads);
+  if (!rc) rc = dev_alloc(&h->d_rel, h->total_beads);
+  if (!rc) rc = dev_alloc(&h->d_centre, h->total_mols);
+  if (!rc) rc = dev_alloc(&h->d_quat, 4 * h->total_mols);
+  if (!rc) rc = dev_alloc(&h->d_mol_start, h->h_mol_start.size());
+  if (!rc) rc = dev_alloc(&h->d_tab, (size_t)kNT * kNT);
+  if (!rc) rc = dev_alloc(&h->d_energy, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_temp_idx, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_slot_of_temp, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_ladder, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_tstep, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_rot_cs, 2 * (size_t)h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_acc_neg, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_acc_boltz, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_rej, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_evals_kh, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_evals_crowd, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_ex_tests, h->n_sys);
+  if (!rc) rc = dev_alloc(&h->d_ex_acc, h->n_sys);
+  if (!rc) rc = dev_alloc(&h->d_ctrl, 4);
+  if (!rc) rc = dev_alloc(&h->d_items, items.size());
+  if (!rc) rc = dev_alloc(&h->d_item_off, item_off.size());
+  if (!rc) rc = dev_alloc(&h->d_scratch, items.size());
+  if (!rc) rc = dev_alloc(&h->d_newpos, h->lmax);
+  if (!rc) rc = dev_alloc(&h->d_dE, 1);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (rc) return;
+    cudaError_t ee = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (ee != cudaSuccess) rc = set_error(REMC_ERR_CUDA, "upload: %s", cudaGetErrorString(ee));
+  };
+  up(h->d_sys, h->h_sys.data(), sizeof(SysDev) * h->h_sys.size());
+  up(h->d_inst_sys, h->h_inst_sys.data(), sizeof(int) * h->n_inst);
+  up(h->d_inst_list, inst_list.data(), sizeof(int) * h->n_inst);
+  up(h->d_mol_start, h->h_mol_start.data(), sizeof(int) * h->h_mol_start.size());
+  up(h->d_items, items.data(), sizeof(TileItem) * items.size());
+  up(h->d_item_off, item_off.data(), sizeof(int) * item_off.size());
+  if (!rc) {
+    cudaMemsetAsync(h->d_acc_neg, 0, sizeof(int) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_acc_boltz, 0, sizeof(int) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_rej, 0, sizeof(int) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_evals_kh, 0, sizeof(unsigned long long) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_evals_crowd, 0, sizeof(unsigned long long) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_ex_tests, 0, sizeof(int) * h->n_sys, h->stream);
+    cudaMemsetAsync(h->d_ex_acc, 0, sizeof(int) * h->n_sys, h->stream);
+    cudaMemsetAsync(h->d_energy, 0, sizeof(double) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_ctrl, 0, sizeof(uint32_t) * 4, h->stream);
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = set_error(REMC_ERR_CUDA, "create sync: %s", cudaGetErrorString(e));
+  }
+  if (rc) {
+    free_all(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return REMC_OK;
+}
+
+int remc_destroy(remc_handle* h) {
+  if (!h) return REMC_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return REMC_OK;
+}
+
+int remc_set_params(remc_handle* h, const remc_params* p) {
+  if (!h || !p) return set_error(REMC_ERR_INVALID, "null argument");
+  if (!(p->debye_length > 0.0f) || (p->crowder_mode != 0 && p->crowder_mode != 1))
+    return set_error(REMC_ERR_INVALID, "bad parameters");
+  h->params = *p;
+  if (h->tables_set) return build_tables(h);
+  return REMC_OK;
+}
+
+int remc_set_type_tables(remc_handle* h, const float* vdw, const float* charge, const float* rho,
+                         const float* pair_table) {
+  if (!h || !vdw || !charge || !rho || !pair_table)
+    return set_error(REMC_ERR_INVALID, "null argument");
+  memcpy(h->vdw, vdw, sizeof(h->vdw));
+  memcpy(h->charge, charge, sizeof(h->charge));
+  memcpy(h->rho, rho, sizeof(h->rho));
+  memcpy(h->pair_table, pair_table, sizeof(h->pair_table));
+  int rc = build_tables(h);
+  if (rc == REMC_OK) h->tables_set = true;
+  return rc;
+}
+
+int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const float* centre,
+                      const double* quat) {
+  if (!h || !pos || !rel || !centre || !quat) return set_error(REMC_ERR_INVALID, "null argument");
+  std::vector<float4> p(h->total_beads), r(h->total_beads), c(h->total_mols);
+  for (int g = 0; g < h->n_inst; ++g) {
+    const int s = h->h_inst_sys[g];
+    const SysDev& S = h->h_sys[s];
+    const int slot = g - S.inst0;
+    const size_t b0 = (size_t)S.bead_base + (size_t)slot * S.n_beads;
+    const size_t m0 = (size_t)S.mol_base + (size_t)slot * S.n_mol;
+    const int* ms = &h->h_mol_start[S.mstart_off];
+    const int* bt = &h->h_bead_type[h->h_bead_off_static[s]];
+    for (int m = 0; m < S.n_mol; ++m) {
+      const size_t gm = m0 + m;
+      for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(centre[3 * gm + k]))
+          return set_error(REMC_ERR_NUMERIC, "instance %d molecule %d: non-finite centre", g, m);
+      c[gm] = make_float4(centre[3 * gm], centre[3 * gm + 1], centre[3 * gm + 2], 0.0f);
+      for (int b = ms[m]; b < ms[m + 1]; ++b) {
+        const size_t gb = b0 + b;
+        for (int k = 0; k < 3; ++k)
+          if (!std::isfinite(pos[3 * gb + k]) || !std::isfinite(rel[3 * gb + k]))
+            return set_error(REMC_ERR_NUMERIC, "instance %d bead %d: non-finite coordinate", g, b);
+        int meta = pack_meta(m, bt[b]);
+        float w;
+        memcpy(&w, &meta, sizeof(w));
+        p[gb] = make_float4(pos[3 * gb], pos[3 * gb + 1], pos[3 * gb + 2], w);
+        r[gb] = make_float4(rel[3 * gb], rel[3 * gb + 1], rel[3 * gb + 2], 0.0f);
+        if (ms[m + 1] - ms[m] == 1 && (rel[3 * gb] != 0.0f || rel[3 * gb + 1] != 0.0f ||
+                                       rel[3 * gb + 2] != 0.0f))
+          return set_error(REMC_ERR_INVALID,
+                           "instance %d molecule %d: a one-bead molecule must sit at its centre",
+                           g, m);
+      }
+    }
+  }
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_pos, p.data(), sizeof(float4) * p.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_rel, r.data(), sizeof(float4) * r.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_centre, c.data(), sizeof(float4) * c.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_quat, quat, sizeof(double) * 4 * h->total_mols,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->state_set = true;
+  return REMC_OK;
+}
+
+int remc_download_state(remc_handle* h, float* pos, float* rel, float* centre, double* quat) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (!h->state_set) return set_error(REMC_ERR_STATE, "state not uploaded");
+  std::vector<float4> p(h->total_beads), r(h->total_beads), c(h->total_mols);
+  REMC_CUDA_TRY(cudaMemcpyAsync(p.data(), h->d_pos, sizeof(float4) * p.size(),
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(r.data(), h->d_rel, sizeof(float4) * r.size(),
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(c.data(), h->d_centre, sizeof(float4) * c.size(),
+                                cudaMemcpyDeviceToHost, h->stream));
+  if (quat)
+    REMC_CUDA_TRY(cudaMemcpyAsync(quat, h->d_quat, sizeof(double) * 4 * h->total_mols,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < h->total_beads; ++i) {
+    if (pos) {
+      pos[3 * i] = p[i].x;
+      pos[3 * i + 1] = p[i].y;
+      pos[3 * i + 2] = p[i].z;
+    }
+    if (rel) {
+      rel[3 * i] = r[i].x;
+      rel[3 * i + 1] = r[i].y;
+      rel[3 * i + 2] = r[i].z;
+    }
+  }
+  if (centre)
+    for (size_t i = 0; i < h->total_mols; ++i) {
+      centre[3 * i] = c[i].x;
+      centre[3 * i + 1] = c[i].y;
+      centre[3 * i + 2] = c[i].z;
+    }
+  return REMC_OK;
+}
+
+int remc_set_replica_params(remc_handle* h, const float* ladder, const float* tstep,
+                            const double* rstep) {
+  if (!h || !ladder || !tstep || !rstep) return set_error(REMC_ERR_INVALID, "null argument");
+  std::vector<int> ti(h->n_inst);
+  std::vector<double> cs(2 * (size_t)h->n_inst);
+  for (int g = 0; g < h->n_inst; ++g) {
+    const SysDev& S = h->h_sys[h->h_inst_sys[g]];
+    if (!(ladder[g] > 0.0f) || !std::isfinite(ladder[g]))
+      return set_error(REMC_ERR_INVALID, "instance %d: temperature must be positive", g);
+    if (g > S.inst0 && !(ladder[g] >= ladder[g - 1]))
+      return set_error(REMC_ERR_INVALID, "ladder must be non-decreasing within a system");
+    ti[g] = g - S.inst0;
+    // Molecule::rotateQ evaluates sin/cos(angle/2.0) in FP64 (Molecule.cpp:290-291)
+    cs[2 * g] = cos(rstep[g] / 2.0);
+    cs[2 * g + 1] = sin(rstep[g] / 2.0);
+  }
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_ladder, ladder, sizeof(float) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_tstep, tstep, sizeof(float) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_rot_cs, cs.data(), sizeof(double) * cs.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_temp_idx, ti.data(), sizeof(int) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  // slot_of_temp is the identity at start (temperature index t held by slot t)
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_slot_of_temp, ti.data(), sizeof(int) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->replica_params_set = true;
+  return REMC_OK;
+}
+
+int remc_energy_full(remc_handle* h, double* out) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
+  int grid = std::min(h->n_items, h->num_sms * 8);
+  energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
+                                                   h->d_items, h->n_items, h->d_scratch,
+                                                   consts_of(h));
+  REMC_CUDA_TRY(cudaGetLastError());
+  energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(h->d_item_off, h->n_inst,
+                                                                  h->d_scratch, h->d_energy);
+  REMC_CUDA_TRY(cudaGetLastError());
+  if (out) {
+    REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_energy, sizeof(double) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+    REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  return REMC_OK;
+}
+
+int remc_get_energies(remc_handle* h, double* out) {
+  if (!h || !out) return set_error(REMC_ERR_INVALID, "null argument");
+  REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_energy, sizeof(double) * h->n_inst,
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
+  if (n_steps == 0) return REMC_OK;
+  return launch_sweep(h, n_steps, seed, step0, nullptr, h->d_inst_list, h->n_inst);
+}
+
+int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
+  for (int s = 0; s < n_steps; ++s) {
+    for (int g = 0; g < h->n_inst; ++g) {
+      // one single-CTA launch per replica per step; d_inst_list + g names one
+      // instance (instances are independent within a step, so order is free)
+      rc = launch_sweep(h, 1, seed, step0 + (uint32_t)s, nullptr, h->d_inst_list + g, 1);
+      if (rc) return rc;
+    }
+  }
+  return REMC_OK;
+}
+
+int remc_exchange(remc_handle* h, uint64_t seed, uint32_t round, int offset) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (offset != 0 && offset != 1) return set_error(REMC_ERR_INVALID, "offset must be 0 or 1");
+  exchange_kernel<<<h->n_sys, 32, 0, h->stream>>>(h->d_sys, h->d_ladder, h->d_energy,
+                                                  h->d_temp_idx, h->d_slot_of_temp,
+                                                  h->d_ex_tests, h->d_ex_acc, nullptr, round,
+                                                  offset, (uint32_t)seed, (uint32_t)(seed >> 32));
+  REMC_CUDA_TRY(cudaGetLastError());
+  return REMC_OK;
+}
+
+int remc_get_temperature_map(remc_handle* h, int* temp_of_slot) {
+  if (!h || !temp_of_slot) return set_error(REMC_ERR_INVALID, "null argument");
+  REMC_CUDA_TRY(cudaMemcpyAsync(temp_of_slot, h->d_temp_idx, sizeof(int) * h->n_inst,
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_get_counters(remc_handle* h, int* accept, int* acceptA, int* reject) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (accept)
+    REMC_CUDA_TRY(cudaMemcpyAsync(accept, h->d_acc_neg, sizeof(int) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (acceptA)
+    REMC_CUDA_TRY(cudaMemcpyAsync(acceptA, h->d_acc_boltz, sizeof(int) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (reject)
+    REMC_CUDA_TRY(cudaMemcpyAsync(reject, h->d_rej, sizeof(int) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_reset_counters(remc_handle* h) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_acc_neg, 0, sizeof(int) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_acc_boltz, 0, sizeof(int) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_rej, 0, sizeof(int) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_evals_kh, 0, sizeof(unsigned long long) * h->n_inst,
+                                h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_evals_crowd, 0, sizeof(unsigned long long) * h->n_inst,
+                                h->stream));
+  return REMC_OK;
+}
+
+int remc_get_pair_evaluations(remc_handle* h, uint64_t* residue_pairs, uint64_t* crowder_pairs) {
+  if (!h || !residue_pairs || !crowder_pairs) return set_error(REMC_ERR_INVALID, "null argument");
+  std::vector<unsigned long long> a(h->n_inst), b(h->n_inst);
+  REMC_CUDA_TRY(cudaMemcpyAsync(a.data(), h->d_evals_kh, sizeof(unsigned long long) * h->n_inst,
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(b.data(), h->d_evals_crowd,
+                                sizeof(unsigned long long) * h->n_inst, cudaMemcpyDeviceToHost,
+                                h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  uint64_t sa = 0, sb = 0;
+  for (int i = 0; i < h->n_inst; ++i) {
+    sa += a[i];
+    sb += b[i];
+  }
+  *residue_pairs = sa;
+  *crowder_pairs = sb;
+  return REMC_OK;
+}
+
+int remc_get_stream(remc_handle* h, void** stream) {
+  if (!h || !stream) return set_error(REMC_ERR_INVALID, "null argument");
+  *stream = (void*)h->stream;
+  return REMC_OK;
+}
+
+int remc_delta_energy(remc_handle* h, int inst, int mol, const float* new_pos, double* dE) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (inst < 0 || inst >= h->n_inst || !new_pos || !dE)
+    return set_error(REMC_ERR_INVALID, "bad instance or null pointer");
+  const int s = h->h_inst_sys[inst];
+  const SysDev& S = h->h_sys[s];
+  if (mol < 0 || mol >= S.n_mol) return set_error(REMC_ERR_INVALID, "bad molecule index");
+  const int* ms = &h->h_mol_start[S.mstart_off];
+  const int n = ms[mol + 1] - ms[mol];
+  std::vector<float4> np(n);
+  for (int k = 0; k < n; ++k) {
+    for (int c = 0; c < 3; ++c)
+      if (!std::isfinite(new_pos[3 * k + c]))
+        return set_error(REMC_ERR_NUMERIC, "non-finite new position");
+    np[k] = make_float4(new_pos[3 * k], new_pos[3 * k + 1], new_pos[3 * k + 2], 0.0f);
+  }
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_newpos, np.data(), sizeof(float4) * n,
+                                cudaMemcpyHostToDevice, h->stream));
+  delta_kernel<<<1, 256, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
+                                         h->d_mol_start, inst, mol, h->d_newpos, h->d_dE,
+                                         consts_of(h));
+  REMC_CUDA_TRY(cudaGetLastError());
+  REMC_CUDA_TRY(cudaMemcpyAsync(dE, h->d_dE, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, uint32_t step0,
+             uint32_t round0) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (n_blocks < 0 || steps_per_block <= 0)
+    return set_error(REMC_ERR_INVALID, "bad block counts");
+  // device control block: step counter, round counter, offset parity
+  uint32_t ctrl[4] = {step0, round0, round0 & 1u, 0u};
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
+  if (!h->graph_exec || h->graph_steps != steps_per_block || h->graph_seed != seed) {
+    if (h->graph_exec) {
+      cudaGraphExecDestroy(h->graph_exec);
+      h->graph_exec = nullptr;
+    }
+    cudaGraph_t graph;
+    REMC_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    rc = launch_sweep(h, steps_per_block, seed, 0, h->d_ctrl, h->d_inst_list, h->n_inst);
+    if (!rc) {
+      exchange_kernel<<<h->n_sys, 32, 0, h->stream>>>(
+          h->d_sys, h->d_ladder, h->d_energy, h->d_temp_idx, h->d_slot_of_temp, h->d_ex_tests,
+          h->d_ex_acc, h->d_ctrl, 0, 0, (uint32_t)seed, (uint32_t)(seed >> 32));
+      ctrl_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_ctrl, (uint32_t)steps_per_block);
+    }
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(REMC_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(REMC_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    h->graph_steps = steps_per_block;
+    h->graph_seed = seed;
+  }
+  for (int b = 0; b < n_blocks; ++b) REMC_CUDA_TRY(cudaGraphLaunch(h->graph_exec, h->stream));
+  return REMC_OK;
+}
+
+int remc_sync(remc_handle* h) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_num_instances(const remc_handle* h) { return h ? h->n_inst : 0; }
+
+}  // extern "C"

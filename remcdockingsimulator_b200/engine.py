@@ -1,0 +1,245 @@
+"""Python mirror of the engine handle (include/remc_b200.h).
+
+`Engine` owns one remc handle: many independent systems, each with its own
+replicas, resident on one GPU. It is the layer the tests and bench drive; the
+C++ facade (csrc/remc_replica.h) offers the same operations under the
+reference's Replica/Molecule names.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import MAX_TYPES, NUM_AMINO, Params, SystemDesc, check, lib
+from .model import System
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def make_params(lambda_: float = 0.159, e0: float = -2.27, debye_length: float = 10.0,
+                crowder_mode: int = 0, crowder_cutoff: float = 15.0,
+                crowder_eps: float = 1.0) -> Params:
+    p = _capi.default_params()
+    p.lambda_ = lambda_
+    p.e0 = e0
+    p.debye_length = debye_length
+    p.crowder_mode = crowder_mode
+    p.crowder_cutoff = crowder_cutoff
+    p.crowder_eps = crowder_eps
+    return p
+
+
+class Engine:
+    """All replicas of all `systems` on one GPU.
+
+    systems[s] is replicated n_replicas[s] times (every replica starts from the
+    system's coordinates unless `upload_state` is called with per-instance
+    arrays). Instances are numbered system-major, slot-minor."""
+
+    def __init__(self, systems: Sequence[System], n_replicas, params: Optional[Params] = None):
+        if isinstance(n_replicas, int):
+            n_replicas = [n_replicas] * len(systems)
+        if len(n_replicas) != len(systems):
+            raise ValueError("one replica count per system")
+        self.systems = list(systems)
+        self.n_replicas = [int(r) for r in n_replicas]
+        self.params = params if params is not None else make_params()
+        table0 = self.systems[0].table
+        for s in self.systems[1:]:
+            if not (np.array_equal(s.table.vdw, table0.vdw) and
+                    np.array_equal(s.table.charge, table0.charge) and
+                    np.array_equal(s.table.pairs, table0.pairs)):
+                raise ValueError("all systems of one engine must share the residue tables")
+        # crowder species: one type per distinct crowder radius
+        radii: List[float] = []
+        for s in self.systems:
+            if any(m.crowder for m in s.molecules) and s.crowder_radius not in radii:
+                radii.append(s.crowder_radius)
+        if len(radii) > MAX_TYPES - NUM_AMINO:
+            raise ValueError("at most %d distinct crowder radii" % (MAX_TYPES - NUM_AMINO))
+        self._species = {r: NUM_AMINO + i for i, r in enumerate(radii)}
+        self._topo = []
+        descs = (SystemDesc * len(self.systems))()
+        for i, s in enumerate(self.systems):
+            mol_start, roles, types = s.topology()
+            if s.crowder_radius in self._species:
+                types = types.copy()
+                types[types >= NUM_AMINO] = self._species[s.crowder_radius]
+            self._topo.append((mol_start, roles, types))
+            d = descs[i]
+            d.n_beads = s.n_beads
+            d.n_mol = s.n_mol
+            d.n_replicas = self.n_replicas[i]
+            d.mol_start = _ptr(mol_start, C.c_int)
+            d.mol_role = _ptr(roles, C.c_int)
+            d.bead_type = _ptr(types, C.c_int)
+            d.box = s.box
+            d.translate_only_crowders = 1 if s.translate_only_crowders else 0
+        h = C.c_void_p()
+        check(lib().remc_create(descs, len(self.systems), C.byref(self.params), C.byref(h)))
+        self._h = h
+        self.n_inst = lib().remc_num_instances(h)
+        self.inst_system = np.repeat(np.arange(len(self.systems)), self.n_replicas)
+        self.inst_slot = np.concatenate([np.arange(r) for r in self.n_replicas])
+        self.inst_first = np.concatenate([[0], np.cumsum(self.n_replicas)[:-1]]).astype(int)
+        self.set_type_tables()
+        self.upload_state()
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().remc_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ set-up
+    def type_tables(self):
+        vdw, q, rho = self.systems[0].type_tables()
+        for r, t in self._species.items():
+            rho[t] = np.float32(r)
+        return vdw, q, rho, np.ascontiguousarray(self.systems[0].table.pairs, np.float32)
+
+    def set_type_tables(self) -> None:
+        vdw, q, rho, pairs = self.type_tables()
+        check(lib().remc_set_type_tables(self._h, _ptr(vdw, C.c_float), _ptr(q, C.c_float),
+                                         _ptr(rho, C.c_float), _ptr(pairs, C.c_float)))
+
+    def set_params(self, params: Params) -> None:
+        self.params = params
+        check(lib().remc_set_params(self._h, C.byref(params)))
+
+    def upload_state(self, pos=None, rel=None, centre=None, quat=None) -> None:
+        """Per-instance state (concatenated in instance order); defaults to
+        every replica holding its system's coordinates."""
+        if pos is None:
+            parts = [[], [], [], []]
+            for s, r in zip(self.systems, self.n_replicas):
+                st = s.state()
+                for k in range(4):
+                    parts[k].extend([st[k]] * r)
+            pos, rel, centre, quat = [np.concatenate(p) for p in parts]
+        pos = np.ascontiguousarray(pos, np.float32)
+        rel = np.ascontiguousarray(rel, np.float32)
+        centre = np.ascontiguousarray(centre, np.float32)
+        quat = np.ascontiguousarray(quat, np.float64)
+        check(lib().remc_upload_state(self._h, _ptr(pos, C.c_float), _ptr(rel, C.c_float),
+                                      _ptr(centre, C.c_float), _ptr(quat, C.c_double)))
+
+    def set_replica_params(self, ladders, translate_steps, rotate_steps) -> None:
+        """ladders: per system, an increasing array of R temperatures;
+        translate/rotate steps: per instance (or per system, broadcast)."""
+        lad = np.concatenate([np.asarray(l, np.float32) for l in ladders]).astype(np.float32)
+        ts = np.asarray(translate_steps, np.float32)
+        rs = np.asarray(rotate_steps, np.float64)
+        if ts.size == len(self.systems):
+            ts = np.repeat(ts, self.n_replicas)
+        if rs.size == len(self.systems):
+            rs = np.repeat(rs, self.n_replicas)
+        ts = np.ascontiguousarray(ts, np.float32)
+        rs = np.ascontiguousarray(rs, np.float64)
+        if lad.size != self.n_inst or ts.size != self.n_inst or rs.size != self.n_inst:
+            raise ValueError("replica parameter arrays must have one entry per instance")
+        check(lib().remc_set_replica_params(self._h, _ptr(lad, C.c_float), _ptr(ts, C.c_float),
+                                            _ptr(rs, C.c_double)))
+        self.ladder = lad
+
+    # ------------------------------------------------------------ compute
+    def energy_full(self) -> np.ndarray:
+        out = np.zeros(self.n_inst, np.float64)
+        check(lib().remc_energy_full(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def energies(self) -> np.ndarray:
+        out = np.zeros(self.n_inst, np.float64)
+        check(lib().remc_get_energies(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def sweep(self, n_steps: int, seed: int, step0: int = 0) -> None:
+        check(lib().remc_sweep(self._h, n_steps, seed, step0))
+
+    def sweep_plain(self, n_steps: int, seed: int, step0: int = 0) -> None:
+        check(lib().remc_sweep_plain(self._h, n_steps, seed, step0))
+
+    def exchange(self, seed: int, round_: int, offset: int) -> None:
+        check(lib().remc_exchange(self._h, seed, round_, offset))
+
+    def run(self, n_blocks: int, steps_per_block: int, seed: int, step0: int = 0,
+            round0: int = 0) -> None:
+        check(lib().remc_run(self._h, n_blocks, steps_per_block, seed, step0, round0))
+
+    def sync(self) -> None:
+        check(lib().remc_sync(self._h))
+
+    def delta_energy(self, inst: int, mol: int, new_pos: np.ndarray) -> float:
+        p = np.ascontiguousarray(new_pos, np.float32).reshape(-1)
+        out = C.c_double(0.0)
+        check(lib().remc_delta_energy(self._h, inst, mol, _ptr(p, C.c_float), C.byref(out)))
+        return out.value
+
+    # ------------------------------------------------------------ read back
+    def download_state(self):
+        nb = sum(s.n_beads * r for s, r in zip(self.systems, self.n_replicas))
+        nm = sum(s.n_mol * r for s, r in zip(self.systems, self.n_replicas))
+        pos = np.zeros((nb, 3), np.float32)
+        rel = np.zeros((nb, 3), np.float32)
+        cen = np.zeros((nm, 3), np.float32)
+        quat = np.zeros((nm, 4), np.float64)
+        check(lib().remc_download_state(self._h, _ptr(pos, C.c_float), _ptr(rel, C.c_float),
+                                        _ptr(cen, C.c_float), _ptr(quat, C.c_double)))
+        return pos, rel, cen, quat
+
+    def instance_slices(self):
+        """(bead slice, molecule slice) of every instance in the flat arrays."""
+        out = []
+        b = m = 0
+        for s, r in zip(self.systems, self.n_replicas):
+            for _ in range(r):
+                out.append((slice(b, b + s.n_beads), slice(m, m + s.n_mol)))
+                b += s.n_beads
+                m += s.n_mol
+        return out
+
+    def temperature_map(self) -> np.ndarray:
+        out = np.zeros(self.n_inst, np.int32)
+        check(lib().remc_get_temperature_map(self._h, _ptr(out, C.c_int)))
+        return out
+
+    def counters(self):
+        a = np.zeros(self.n_inst, np.int32)
+        b = np.zeros(self.n_inst, np.int32)
+        r = np.zeros(self.n_inst, np.int32)
+        check(lib().remc_get_counters(self._h, _ptr(a, C.c_int), _ptr(b, C.c_int),
+                                      _ptr(r, C.c_int)))
+        return a, b, r
+
+    def reset_counters(self) -> None:
+        check(lib().remc_reset_counters(self._h))
+
+    def pair_evaluations(self):
+        """(residue-residue, crowder) pair evaluations since the last reset."""
+        a = C.c_uint64(0)
+        b = C.c_uint64(0)
+        check(lib().remc_get_pair_evaluations(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        s = C.c_void_p(0)
+        check(lib().remc_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
