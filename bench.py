@@ -117,76 +117,42 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- reference CPU
-def reference_exe():
-    from oracle import bindings as ob
-    return ob.REF_EXE if os.path.exists(ob.REF_EXE) else None
+PAIRS_PER_CORE_S = 2.5e7  # order of the reference E() rate per core (pairs/s)
 
 
-def run_reference_sample(workload, systems, mc_steps: int, resteps: int, cores: int):
-    """Run the reference CPU engine on the given system indices concurrently
-    (one process per system, threads dividing the replica count). Returns
-    (replica_steps, seconds, threads_used, detail)."""
-    exe = reference_exe()
-    if exe is None:
-        raise RuntimeError("reference engine not built (oracle/_ref/REMCDockingCPU)")
-    from remcdockingsimulator_b200 import synth
-    work = tempfile.mkdtemp(prefix="remc_ref_")
-    procs = []
-    threads_used = 0
-    try:
-        per = []
-        for si in systems:
-            R = workload.n_replicas[si]
-            t = R
-            while t > 1 and (t > cores or R % t):
-                t -= 1
-            d = os.path.join(work, "sys%03d" % si)
-            cfg = synth.write_reference_inputs(workload, si, d, mc_steps, resteps, t)
-            per.append((si, d, cfg, t, R))
-        # as many concurrent processes as the cores allow
-        slots = max(1, cores // max(p[3] for p in per))
-        env = dict(os.environ)
-        env["LD_LIBRARY_PATH"] = "/usr/local/cuda/lib64:" + env.get("LD_LIBRARY_PATH", "")
-        t0 = time.perf_counter()
-        pending = list(per)
-        running = []
-        sim_ms = []
-        rsteps = 0
-        while pending or running:
-            while pending and len(running) < slots:
-                si, d, cfg, t, R = pending.pop(0)
-                p = subprocess.Popen([exe, "-f", cfg, "-t", str(t)], cwd=d, env=env,
-                                     stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
-                running.append((p, R))
-                threads_used = max(threads_used, t * min(slots, len(per)))
-            for p, R in list(running):
-                if p.poll() is not None:
-                    out = p.stdout.read()
-                    if p.returncode != 0:
-                        raise RuntimeError("reference engine failed:\n" + out[-2000:])
-                    m = re.search(r"Simulation:\s+([0-9.]+) ms", out)
-                    if m:
-                        sim_ms.append(float(m.group(1)))
-                    rsteps += R * mc_steps
-                    running.remove((p, R))
-            time.sleep(0.01)
-        wall = time.perf_counter() - t0
-    finally:
-        shutil.rmtree(work, ignore_errors=True)
-    return rsteps, wall, threads_used, {"sim_ms": sim_ms, "processes": len(systems),
-                                        "concurrent": slots}
-
-
-def reference_sample_plan(workload, seed: int):
+def reference_sample_plan(workload, seed: int, cores: int, seconds: float):
+    """Pick up to 8 systems of the workload (seeded) and an MC step count so
+    that one sample is about `seconds` of work for `cores` threads of the
+    reference engine, which evaluates the full O(N^2) energy every step."""
     import numpy as np
     n = len(workload.systems)
     rng = np.random.default_rng(seed + 777)
     k = min(n, 8)
     systems = sorted(rng.choice(n, size=k, replace=False).tolist())
-    pairs_per_step = sum(workload.systems[i].n_beads ** 2 / 2 for i in systems) / k
-    # ~28e6 pair evaluations/s per core for the reference E() (measured order)
-    mc = max(4, min(200, int(2.0e7 / max(pairs_per_step, 1.0))))
-    return systems, mc
+    pairs = sum(workload.n_replicas[i] * workload.systems[i].n_beads ** 2 / 2.0 for i in systems)
+    mc = int(PAIRS_PER_CORE_S * cores * seconds / max(pairs, 1.0))
+    return systems, max(2, min(mc, 2000))
+
+
+def build_reference_replicas(workload, systems):
+    """The reference's own Replica objects (oracle/_ref, compiled from its
+    sources) for every replica of the sampled systems; the reference
+    executable itself cannot load more than 30 molecules (double free in
+    Replica::loadMolecule), so the replicas are built through the harness."""
+    from oracle import bindings as ob
+    reps = []
+    for si in systems:
+        s = workload.systems[si]
+        for T in workload.ladders[si]:
+            r = ob.ReferenceReplica(s, temperature=float(T))
+            r.set_steps(workload.translate_step, workload.rotate_step)
+            reps.append(r)
+    return reps
+
+
+def time_reference(reps, threads: int, mc: int):
+    from oracle import bindings as ob
+    return ob.time_reference_mcsearch(reps, threads, mc)
 
 
 # ---------------------------------------------------------------- our arm
@@ -387,15 +353,19 @@ def main():
 def cpu_baseline(workload, seed: int):
     cores = os.cpu_count() or 1
     try:
-        systems, mc = reference_sample_plan(workload, seed)
-        rsteps, wall, threads, detail = run_reference_sample(workload, systems, mc, 2, cores)
-        return {"value": rsteps / wall, "unit": "replica-steps/s", "cores": threads,
+        systems, mc = reference_sample_plan(workload, seed, cores, 10.0)
+        reps = build_reference_replicas(workload, systems)
+        wall = time_reference(reps, cores, mc)
+        n_rs = len(reps) * mc
+        for r in reps:
+            r.close()
+        return {"value": n_rs / wall, "unit": "replica-steps/s", "cores": min(cores, len(reps)),
                 "kind": "reference",
-                "sample": "reference REMCDockingCPU on %d of %d systems x all replicas x %d MC "
-                          "steps (full energy per step, its own (6/r)^6 crowder model and "
-                          "lambda=0.159), wall time incl. start-up" % (len(systems),
-                                                                    len(workload.systems), mc),
-                "detail": detail}
+                "sample": "reference Replica::MCSearch (compiled from its sources, full energy "
+                          "every step, its own (6/r)^6 crowder model and lambda=0.159) on all "
+                          "%d replicas of %d of %d systems x %d MC steps, %d threads, %.1f s" %
+                          (len(reps), len(systems), len(workload.systems), mc,
+                           min(cores, len(reps)), wall)}
     except Exception as exc:  # reported, not fatal: the GPU number stands alone
         return {"value": None, "unit": "replica-steps/s", "cores": 0, "kind": "reference",
                 "sample": "failed: %s" % str(exc)[:300]}
@@ -404,38 +374,39 @@ def cpu_baseline(workload, seed: int):
 def reference_arm(args, world: int, rank: int):
     if rank != 0:
         return 0
-    from remcdockingsimulator_b200 import synth
-    exe = reference_exe()
-    if exe is None:
+    from oracle import bindings as ob
+    if not ob.reference_available():
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU engine not built in oracle/_ref"}))
         return 0
+    from remcdockingsimulator_b200 import synth
     w = synth.WORKLOADS[args.workload](args.seed)
     cores = os.cpu_count() or 1
-    systems, mc = reference_sample_plan(w, args.seed)
+    systems, mc = reference_sample_plan(w, args.seed, cores, 4.0)
+    reps = build_reference_replicas(w, systems)
+    threads = min(cores, len(reps))
     for _ in range(args.warmup):
-        run_reference_sample(w, systems[:1], max(2, mc // 4), 1, cores)
-    total_rs = 0
+        time_reference(reps, threads, max(1, mc // 8))
     total_t = 0.0
-    threads = 0
     for _ in range(args.steps):
-        rs, wall, threads, detail = run_reference_sample(w, systems, mc, 2, cores)
-        total_rs += rs
-        total_t += wall
-    value = total_rs / total_t
+        total_t += time_reference(reps, threads, mc)
+    for r in reps:
+        r.close()
+    value = len(reps) * mc * args.steps / total_t
     line = {
         "impl": "reference",
         "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",
         "value": value, "unit": "replica-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_t * 1000.0 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-        "data": "synthetic (seeded generator, written in the reference's config/PDB formats)",
+        "data": "synthetic (seeded generator with the benchmark configuration's shapes)",
         "config": {"workload": w.name, "description": w.description,
                    "sample_systems": systems, "mc_steps_per_sample": mc},
         "cpu_baseline": {"value": value, "unit": "replica-steps/s", "cores": threads,
                          "kind": "reference",
-                         "sample": "%d systems x all replicas x %d MC steps per bench step" %
-                                   (len(systems), mc)},
+                         "sample": "reference Replica::MCSearch on all %d replicas of %d of %d "
+                                   "systems x %d MC steps per bench step, %d threads" %
+                                   (len(reps), len(systems), len(w.systems), mc, threads)},
         "e2e": {"value": value, "unit": "replica-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

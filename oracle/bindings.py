@@ -241,6 +241,8 @@ def ref_lib():
         L.ref_replica_mcsearch.argtypes = [C.c_void_p, C.c_int, PD, PI, PI, PD]
         L.ref_replica_mcsearch.restype = C.c_int
         L.ref_random_vectors.argtypes = [C.c_void_p, PD, PF, PD]
+        L.ref_time_mcsearch.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int]
+        L.ref_time_mcsearch.restype = C.c_double
         _rlib = L
     return _rlib
 
@@ -312,6 +314,9 @@ class ReferenceReplica:
                                         _p(cen, C.c_float), _p(quat, C.c_double))
         return pos, rel, cen, quat
 
+    def steps_set(self, translate_step: float, rotate_step: float) -> None:
+        self.set_steps(translate_step, rotate_step)
+
     def mcsearch(self, u: np.ndarray):
         """Run len(u) reference MCSearch steps fed with u[s] = 6 uniforms."""
         u = np.ascontiguousarray(u, np.float64).reshape(-1, 6)
@@ -322,3 +327,10 @@ class ReferenceReplica:
         under = ref_lib().ref_replica_mcsearch(self.h, n, _p(u, C.c_double), _p(flags, C.c_int),
                                                _p(mol, C.c_int), _p(en, C.c_double))
         return flags, mol, en, under
+
+
+def time_reference_mcsearch(replicas, n_threads: int, n_steps: int) -> float:
+    """Wall seconds of the reference's own MCSearch(n_steps) on every replica,
+    spread over n_threads host threads."""
+    arr = (C.c_void_p * len(replicas))(*[r.h for r in replicas])
+    return ref_lib().ref_time_mcsearch(arr, len(replicas), n_threads, n_steps)

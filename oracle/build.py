@@ -32,7 +32,8 @@ REF_UNITS = ["AminoAcid", "AminoAcids", "Link", "Molecule", "Quaternion", "Repli
              "TorsionalLookupMatrix", "vector3f"]
 # the reference's own CPU flags (simulation engine/Makefile:17); gnu++11 only
 # because the stubs use <chrono>; -fpermissive for its pre-standard C++.
-REF_CFLAGS = ["-std=gnu++11", "-fpermissive", "-w", "-O2", "-fno-omit-frame-pointer", "-fPIC"]
+REF_CFLAGS = ["-std=gnu++11", "-fpermissive", "-w", "-O2", "-fno-omit-frame-pointer", "-fPIC",
+              "-pthread"]
 
 
 def _run(cmd: list[str]) -> None:
@@ -87,7 +88,7 @@ def build_reference(force: bool = False) -> bool:
     lib = os.path.join(REF_OUT, "libremcref.so")
     lib_objs = [o for o in objs if not o.endswith("main.o")] + [harness_obj]
     if force or _stale(lib, lib_objs):
-        _run(["g++", "-shared", "-o", lib] + lib_objs + ["-lpthread"])
+        _run(["g++", "-shared", "-pthread", "-o", lib] + lib_objs + ["-lpthread"])
     exe = os.path.join(REF_OUT, "REMCDockingCPU")
     main_objs = [o for o in objs]
     if force or _stale(exe, main_objs):

@@ -15,9 +15,11 @@
 //   * run the reference's own `Replica::MCSearch` (Replica.cpp:368-478) one step
 //     at a time, with its GSL generators fed from a caller-supplied uniform
 //     stream (the shared Philox stream), and report every accept/reject.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #define private public  // Replica::translate/rotate are private; the harness probes them
@@ -244,6 +246,39 @@ void ref_random_vectors(void* hp, const double* u3, float* vf, double* vd) {
   gsl_rng_free(r);
   vf[0] = a.x; vf[1] = a.y; vf[2] = a.z;
   vd[0] = b.x; vd[1] = b.y; vd[2] = b.z;
+}
+
+// Timing driver for the CPU baseline: the reference's own Replica::MCSearch
+// (Replica.cpp:368-478, full Replica::E() every step, MT19937 draws) on
+// `n` replicas spread over `n_threads` host threads, replicas assigned to
+// threads in contiguous slices as MCthreadableFunction does
+// (main.cpp:879-883). The replicas must not be in fed mode. Returns wall
+// seconds. (The reference executable itself cannot load more than 30
+// molecules: Replica::loadMolecule grows its array with a shallow memcpy and
+// the deleted originals free the file names the copies still hold.)
+double ref_time_mcsearch(void** handles, int n, int n_threads, int n_steps) {
+  if (n_threads < 1) n_threads = 1;
+  if (n_threads > n) n_threads = n;
+  for (int i = 0; i < n; ++i) {
+    Replica& r = ((Harness*)handles[i])->rep;
+    gsl_rng* all[7] = {r.rng_moleculeSelection, r.MCRng, r.rng_rotate, r.rng_translate,
+                       r.MCKbRng, r.rng_rotateAmount, r.rng_translateAmount};
+    for (int k = 0; k < 7; ++k) {
+      all[k]->fed = 0;
+      gsl_rng_set(all[k], 1000u + 7u * (unsigned)i + (unsigned)k);
+    }
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  const int per = (n + n_threads - 1) / n_threads;
+  for (int t = 0; t < n_threads; ++t) {
+    pool.emplace_back([=]() {
+      for (int i = t * per; i < n && i < (t + 1) * per; ++i)
+        ((Harness*)handles[i])->rep.MCSearch(n_steps);
+    });
+  }
+  for (auto& th : pool) th.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 }  // extern "C"

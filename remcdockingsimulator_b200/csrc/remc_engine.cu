@@ -831,13 +831,20 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   int max_smem = 0;
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  if (smem > (size_t)max_smem) {
+  cudaFuncAttributes fattr;
+  e = cudaFuncGetAttributes(&fattr, sweep_kernel);
+  if (e != cudaSuccess) {
+    delete h;
+    return set_error(REMC_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+  }
+  const int max_dyn = max_smem - (int)fattr.sharedSizeBytes;
+  if (smem > (size_t)max_dyn) {
     delete h;
     return set_error(REMC_ERR_INVALID,
                      "largest system needs %zu bytes of shared memory, device allows %d", smem,
-                     max_smem);
+                     max_dyn);
   }
-  e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn);
   if (e != cudaSuccess) {
     delete h;
     return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
@@ -1196,8 +1203,8 @@ int remc_get_stream(remc_handle* h, void** stream) {
 }
 
 int remc_delta_energy(remc_handle* h, int inst, int mol, const float* new_pos, double* dE) {
-  int rc = check_ready(h);
-  if (rc) return rc;
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   if (inst < 0 || inst >= h->n_inst || !new_pos || !dE)
     return set_error(REMC_ERR_INVALID, "bad instance or null pointer");
   const int s = h->h_inst_sys[inst];
