@@ -67,16 +67,71 @@ struct SysDev {
   int n_chain_beads;  // beads of residue type; the rest are crowders
 };
 
-// Per-step proposal data computed 32 steps at a time by warp 0.
-struct StepInfo {
+// Per-step proposal record: everything about step s of one replica that does
+// not depend on the replica's state (Philox draws, chosen molecule, move type,
+// translation vector, step quaternion). Written by proposal_kernel for a
+// whole sweep, streamed through shared memory by sweep_kernel.
+struct StepRec {
   double q[4];      // step quaternion (rotation)
   double u5;        // Metropolis uniform
   float t[3];       // translation vector
   int m;            // molecule
   int rotate;       // 1 rotation, 0 translation
-  int pad;
+  int crowd;        // 1 if the molecule is a crowder
 };
-static_assert(sizeof(StepInfo) == 64, "StepInfo layout");
+static_assert(sizeof(StepRec) == 64, "StepRec layout");
+
+struct ProposalArgs {
+  const SysDev* sys;
+  const int* inst_sys;
+  const int* mol_start;
+  const int* mol_role;
+  const int* mrole_off;  // per system: offset of its roles in mol_role
+  const float* tstep;
+  const double* rot_cs;
+  StepRec* recs;         // [n_inst][rec_stride]
+  const uint32_t* ctrl;
+  uint32_t step0;
+  uint32_t seed_lo, seed_hi;
+  int n_inst, n_steps, rec_stride;
+};
+
+// One thread per (instance, step): Replica::MCSearch's choices for that step
+// (Replica.cpp:384-402) from the counter-based stream.
+__global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)P.n_inst * P.n_steps) return;
+  const int inst = (int)(idx / P.n_steps), s = (int)(idx % P.n_steps);
+  const int sysid = P.inst_sys[inst];
+  const SysDev S = P.sys[sysid];
+  const int slot = inst - S.inst0;
+  const uint32_t step = (P.ctrl ? P.ctrl[0] : P.step0) + (uint32_t)s;
+  uint4 c = make_uint4(step, (uint32_t)slot, (uint32_t)sysid, 0u);
+  const uint2 k = make_uint2(P.seed_lo, P.seed_hi);
+  const uint4 x = philox4x32_10(c, k);
+  c.w = 1u;
+  const uint4 y = philox4x32_10(c, k);
+  const double u0 = u32_unit(x.x), u1 = u32_unit(x.y), u2 = u32_unit(x.z), u3 = u32_unit(x.w);
+  const double u4 = u32_unit(y.x), u5 = u32_unit(y.y);
+  StepRec r;
+  r.m = (int)__dmul_rn(u0, (double)S.n_mol);
+  const bool crowd = P.mol_role[P.mrole_off[sysid] + r.m] == -1;
+  r.rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
+  r.u5 = u5;
+  if (r.rotate) {
+    step_quaternion(u2, u3, u4, P.rot_cs[2 * inst], P.rot_cs[2 * inst + 1], r.q);
+    r.t[0] = r.t[1] = r.t[2] = 0.0f;
+  } else {
+    const float3 t = translate_vector(u2, u3, u4, P.tstep[inst]);
+    r.t[0] = t.x;
+    r.t[1] = t.y;
+    r.t[2] = t.z;
+    r.q[0] = 1.0;
+    r.q[1] = r.q[2] = r.q[3] = 0.0;
+  }
+  r.crowd = crowd ? 1 : 0;
+  P.recs[(size_t)inst * P.rec_stride + s] = r;
+}
 
 struct SweepArgs {
   const SysDev* sys;
@@ -88,28 +143,27 @@ struct SweepArgs {
   double* quat;
   const int* mol_start;
   const float4* tab;
+  const StepRec* recs;   // [n_inst][rec_stride]
   double* energy;
   const int* temp_idx;
   const float* ladder;
-  const float* tstep;
-  const double* rot_cs;  // cos, sin of the half rotate step per instance
   int* acc_neg;          // accepted with dE < 0
   int* acc_boltz;        // accepted by the Boltzmann test
   int* rej;
   unsigned long long* evals_kh;     // residue-residue pair evaluations
   unsigned long long* evals_crowd;  // pair evaluations involving a crowder
-  const uint32_t* ctrl;  // device step counter (graph mode) or null
-  uint32_t step0;
-  uint32_t seed_lo, seed_hi;
+  int rec_stride, rec_offset;       // records of step s at rec_offset + s
   int n_steps;
   int nmax, mmax, lmax;  // shared-memory capacities
   EnergyConsts K;
 };
 
+constexpr int kRing = 64;  // proposal records held in shared memory (two halves)
+
 // Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
-// mmax molecules, lmax beads per molecule, nwarps).
+// mmax molecules, lmax beads per molecule).
 struct SweepSmem {
-  size_t tab, beads, centres, trial_pos, trial_rel, mstart, info, red, total;
+  size_t tab, beads, centres, trial_pos, mstart, ring, red, total;
   static __host__ __device__ size_t take(size_t& off, size_t bytes) {
     size_t o = off;
     off += (bytes + 15) & ~size_t(15);
@@ -122,35 +176,42 @@ struct SweepSmem {
     s.beads = take(off, sizeof(float4) * nmax);
     s.centres = take(off, sizeof(float4) * mmax);
     s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
-    s.trial_rel = take(off, sizeof(float4) * 2 * lmax);
     s.mstart = take(off, sizeof(int) * (mmax + 1));
-    s.info = take(off, sizeof(StepInfo) * 32);
-    s.red = take(off, sizeof(double) * 32 + 64);
+    s.ring = take(off, sizeof(StepRec) * kRing);
+    s.red = take(off, sizeof(double) * 2 * 32);
     s.total = off;
     return s;
   }
 };
 
-// Control block written by thread 0 each step, read by all after a barrier.
-struct StepCtl {
-  float nc[3];
-  int m0, n_m, rotate, skip, buf;
-  // previous step (applied at the start of this step)
-  int p_acc, p_m0, p_n, p_rot, p_buf;
-};
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n"); }
 
-__global__ void __launch_bounds__(512) sweep_kernel(SweepArgs A) {
+// One CTA per replica-instance, persistent over the sweep. The instance's beads
+// and molecule centres stay in shared memory for all n_steps steps.
+//
+// Ownership: in the pair loop thread t reads only beads j = t (mod T), and the
+// same thread writes those beads when a move is accepted, so bead updates need
+// no barrier. Every thread computes the FP64 sum of the per-warp partials and
+// the Metropolis decision itself (same order, same result), and tracks the
+// previous step's move to read a molecule moved one step ago from registers or
+// the trial buffer rather than from another thread's not-yet-ordered write.
+// A step of a one-bead molecule therefore costs one barrier; a chain step
+// costs two (trial positions are built by the owners of the chain's beads).
+__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
   float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
   float4* s_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
-  float4* s_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
   int* s_mstart = reinterpret_cast<int*>(smem_raw + L.mstart);
-  StepInfo* s_info = reinterpret_cast<StepInfo*>(smem_raw + L.info);
+  StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
-  __shared__ StepCtl ctl;
 
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
@@ -162,214 +223,200 @@ __global__ void __launch_bounds__(512) sweep_kernel(SweepArgs A) {
   const int bead_off = S.bead_base + slot * N;
   const int mol_off = S.mol_base + slot * M;
   const float box = S.box, invbox = S.invbox;
-  const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
+  const StepRec* recs = A.recs + (size_t)inst * A.rec_stride + A.rec_offset;
+  const int n_steps = A.n_steps;
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
   for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
   for (int i = tid; i < M; i += nthr) s_cent[i] = A.centre[mol_off + i];
   for (int i = tid; i <= M; i += nthr) s_mstart[i] = A.mol_start[S.mstart_off + i];
-
+  {
+    // first ring fill: records of steps 0..min(kRing, n_steps)-1, 16 B per copy
+    const int nrec = min(kRing, n_steps);
+    const int chunks = nrec * (int)(sizeof(StepRec) / 16);
+    for (int c = tid; c < chunks; c += nthr)
+      cp_async16(reinterpret_cast<char*>(s_ring) + 16 * c,
+                 reinterpret_cast<const char*>(recs) + 16 * c);
+    cp_async_commit();
+    cp_async_wait_all();
+  }
   const float T = A.ladder[S.inst0 + A.temp_idx[inst]];
-  const float tstep = A.tstep[inst];
-  const double cosa = A.rot_cs[2 * inst], sina = A.rot_cs[2 * inst + 1];
+  const double beta = 4184.0 / ((double)8.314472f * (double)T);
   double energy = 0.0;
   int n_neg = 0, n_boltz = 0, n_rej = 0;
   unsigned long long ev_kh = 0, ev_crowd = 0;
-  if (tid == 0) {
-    energy = A.energy[inst];
-    ctl.p_acc = 0;
-  }
-  const double beta = 4184.0 / ((double)8.314472f * (double)T);
+  if (tid == 0) energy = A.energy[inst];
   __syncthreads();
 
-  for (int s = 0; s < A.n_steps; ++s) {
-    // ---- warp 0: proposals for the next 32 steps (Philox + normalisations)
-    if (warp == 0) {
-      if ((s & 31) == 0) {
-        int st = s + lane;
-        if (st < A.n_steps) {
-          uint4 c = make_uint4(step0 + (uint32_t)st, (uint32_t)slot, (uint32_t)sysid, 0u);
-          uint2 k = make_uint2(A.seed_lo, A.seed_hi);
-          uint4 x = philox4x32_10(c, k);
-          c.w = 1u;
-          uint4 y = philox4x32_10(c, k);
-          double u0 = u32_unit(x.x), u1 = u32_unit(x.y), u2 = u32_unit(x.z), u3 = u32_unit(x.w);
-          double u4 = u32_unit(y.x), u5 = u32_unit(y.y);
-          StepInfo inf;
-          inf.m = (int)__dmul_rn(u0, (double)M);
-          int crowd = bead_type(s_beads[s_mstart[inf.m]].w) >= kNumAmino;
-          inf.rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
-          inf.u5 = u5;
-          if (inf.rotate) {
-            step_quaternion(u2, u3, u4, cosa, sina, inf.q);
-            inf.t[0] = inf.t[1] = inf.t[2] = 0.0f;
-          } else {
-            float3 t = translate_vector(u2, u3, u4, tstep);
-            inf.t[0] = t.x;
-            inf.t[1] = t.y;
-            inf.t[2] = t.z;
-            inf.q[0] = 1.0;
-            inf.q[1] = inf.q[2] = inf.q[3] = 0.0;
-          }
-          inf.pad = 0;
-          s_info[lane] = inf;
-        }
-        __syncwarp();
-      }
-      if (lane == 0) {
-        const StepInfo& inf = s_info[s & 31];
-        int m = inf.m;
-        int m0 = s_mstart[m], n = s_mstart[m + 1] - m0;
-        float4 c = s_cent[m];
-        float nc0 = c.x, nc1 = c.y, nc2 = c.z;
-        if (!inf.rotate) {
-          nc0 = fmodf(__fadd_rn(__fadd_rn(c.x, inf.t[0]), box), box);
-          nc1 = fmodf(__fadd_rn(__fadd_rn(c.y, inf.t[1]), box), box);
-          nc2 = fmodf(__fadd_rn(__fadd_rn(c.z, inf.t[2]), box), box);
-        }
-        ctl.nc[0] = nc0;
-        ctl.nc[1] = nc1;
-        ctl.nc[2] = nc2;
-        ctl.m0 = m0;
-        ctl.n_m = n;
-        ctl.rotate = inf.rotate;
-        ctl.skip = inf.rotate && n == 1;  // a one-bead rotation moves nothing: dE = 0
-        ctl.buf = s & 1;
-      }
-    }
-    __syncthreads();  // A: proposal ready, previous decision visible
+  // previous step, known to every thread
+  int p_m = -1, p_acc = 0, p_rot = 0, p_n = 0, p_b = 0;
+  float4 p_single = make_float4(0.f, 0.f, 0.f, 0.f);  // accepted one-bead position
+  float p_nc0 = 0.f, p_nc1 = 0.f, p_nc2 = 0.f;          // accepted new centre
 
-    // ---- apply the previous accepted move, build this step's trial positions
-    {
-      const int m0 = ctl.m0, n = ctl.n_m, rot = ctl.rotate, b = ctl.buf;
-      const int pacc = ctl.p_acc, pm0 = ctl.p_m0, pn = ctl.p_n, prot = ctl.p_rot, pb = ctl.p_buf;
-      if (pacc) {
-        for (int k = tid; k < pn; k += nthr) {
-          s_beads[pm0 + k] = s_tpos[pb * A.lmax + k];
-          if (prot && pn > 1) A.rel[bead_off + pm0 + k] = s_trel[pb * A.lmax + k];
-        }
-      }
-      const float nc0 = ctl.nc[0], nc1 = ctl.nc[1], nc2 = ctl.nc[2];
-      if (rot) {
-        if (n > 1) {
-          const StepInfo& inf = s_info[s & 31];
-          QuatProducts qp = quat_products(inf.q[0], inf.q[1], inf.q[2], inf.q[3]);
-          for (int k = tid; k < n; k += nthr) {
-            float4 rl = A.rel[bead_off + m0 + k];
-            float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
-            float w = s_beads[m0 + k].w;
-            s_trel[b * A.lmax + k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
-            s_tpos[b * A.lmax + k] =
-                make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
-          }
-        } else if (tid == 0) {
-          s_tpos[b * A.lmax] = s_beads[m0];
-        }
-      } else {
-        for (int k = tid; k < n; k += nthr) {
-          float4 rl = (n > 1) ? A.rel[bead_off + m0 + k] : make_float4(0.f, 0.f, 0.f, 0.f);
-          float w = s_beads[m0 + k].w;
-          s_tpos[b * A.lmax + k] =
-              make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
-        }
-      }
+  for (int s = 0; s < n_steps; ++s) {
+    // ---- prefetch the next ring half (records s+32 .. s+63)
+    if ((s & 31) == 0 && s > 0 && s + 32 < n_steps) {
+      const int first = s + 32;
+      const int nrec = min(32, n_steps - first);
+      const int chunks = nrec * (int)(sizeof(StepRec) / 16);
+      char* dst = reinterpret_cast<char*>(s_ring + (first & (kRing - 1)));
+      const char* src = reinterpret_cast<const char*>(recs + first);
+      for (int c = tid; c < chunks; c += nthr) cp_async16(dst + 16 * c, src + 16 * c);
+      cp_async_commit();
     }
-    __syncthreads();  // T: beads current, trial ready
+    const StepRec rec = s_ring[s & (kRing - 1)];
+    const int m = rec.m;
+    const int m0 = s_mstart[m], n = s_mstart[m + 1] - m0;
+    const int b = s & 1;
+    const bool same = (m == p_m) && p_acc;  // moved (and accepted) last step
+    // centre of m: the one this step's thread computed last step if m moved then
+    float c0, c1, c2;
+    if (same && !p_rot) {
+      c0 = p_nc0;
+      c1 = p_nc1;
+      c2 = p_nc2;
+    } else {
+      const float4 c = s_cent[m];
+      c0 = c.x;
+      c1 = c.y;
+      c2 = c.z;
+    }
+    float nc0 = c0, nc1 = c1, nc2 = c2;
+    if (!rec.rotate) {
+      nc0 = fmodf(__fadd_rn(__fadd_rn(c0, rec.t[0]), box), box);
+      nc1 = fmodf(__fadd_rn(__fadd_rn(c1, rec.t[1]), box), box);
+      nc2 = fmodf(__fadd_rn(__fadd_rn(c2, rec.t[2]), box), box);
+    }
+    // a one-bead rotation moves nothing (its bead sits at the centre): dE = 0
+    const bool skip = rec.rotate && n == 1;
+    float4 pold1, pnew1;  // one-bead molecule: old/new position in registers
+    if (n == 1) {
+      pold1 = same ? p_single : s_beads[m0];
+      pnew1 = make_float4(nc0, nc1, nc2, pold1.w);
+    } else {
+      // trial positions of the chain, built by the owners of its beads
+      QuatProducts qp{};
+      if (rec.rotate) qp = quat_products(rec.q[0], rec.q[1], rec.q[2], rec.q[3]);
+      int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
+      for (; j < m0 + n; j += nthr) {
+        const int k = j - m0;
+        const float4 rl = A.rel[bead_off + j];
+        const float w = s_beads[j].w;
+        float4 np;
+        if (rec.rotate) {
+          const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
+          np = make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
+        } else {
+          np = make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
+        }
+        s_tpos[b * A.lmax + k] = np;
+      }
+      __syncthreads();  // trial positions and the previous chain update visible
+    }
 
-    // ---- dE = sum over beads k of the molecule, beads j outside it
+    // ---- dE over beads j outside the molecule (thread t owns j = t mod T)
     double dacc = 0.0;
-    if (!ctl.skip) {
-      const int m0 = ctl.m0, n = ctl.n_m, b = ctl.buf;
-      const int nrest = N - n;
+    if (!skip) {
       for (int k = 0; k < n; ++k) {
-        const float4 pold = s_beads[m0 + k];
-        const float4 pnew = s_tpos[b * A.lmax + k];
+        float4 pold, pnew;
+        if (n == 1) {
+          pold = pold1;
+          pnew = pnew1;
+        } else {
+          pold = (same) ? s_tpos[p_b * A.lmax + k] : s_beads[m0 + k];
+          pnew = s_tpos[b * A.lmax + k];
+        }
         const int ta = bead_type(pold.w);
         const bool a_crowd = ta >= kNumAmino;
         const float4* trow = s_tab + ta * kNT;
         float acc = 0.0f;
-        for (int jj = tid; jj < nrest; jj += nthr) {
-          const int j = jj < m0 ? jj : jj + n;
+        for (int j = tid; j < N; j += nthr) {
+          if (j >= m0 && j < m0 + n) continue;
           const float4 pj = s_beads[j];
           const int tb = bead_type(pj.w);
           const float4 Tj = trow[tb];
           const bool crowd = a_crowd || tb >= kNumAmino;
-          float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
-          float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
+          const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
+          const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
           acc += en - eo;
         }
         dacc += (double)acc;
       }
     }
     dacc = warp_sum(dacc);
-    if (lane == 0) s_red[warp] = dacc;
-    __syncthreads();  // R: partial sums ready
+    if (lane == 0) s_red[b * 32 + warp] = dacc;
+    if ((s & 31) == 31) cp_async_wait_all();  // next ring half has landed
+    __syncthreads();  // R: partial sums (and the prefetched records) visible
 
-    // ---- warp 0: reduce, Metropolis, bookkeeping
-    if (warp == 0) {
-      double v = lane < nwarps ? s_red[lane] : 0.0;
-      v = warp_sum(v);
-      if (lane == 0) {
-        const StepInfo& inf = s_info[s & 31];
-        const double dE = v;
-        if (!ctl.skip) {
-          // two evaluations (old and new position) per pair
-          const unsigned long long n = (unsigned long long)ctl.n_m;
-          if (bead_type(s_beads[ctl.m0].w) >= kNumAmino) {
-            ev_crowd += 2ull * n * (unsigned long long)(N - ctl.n_m);
-          } else {
-            ev_kh += 2ull * n * (unsigned long long)(S.n_chain_beads - ctl.n_m);
-            ev_crowd += 2ull * n * (unsigned long long)(N - S.n_chain_beads);
+    // ---- every thread: the same FP64 sum and the same Metropolis decision
+    double dE = 0.0;
+    for (int w = 0; w < nwarps; ++w) dE += s_red[b * 32 + w];
+    int acc = 0;
+    if (dE < 0.0) {
+      acc = 1;
+    } else if (rec.u5 < exp(-dE * beta)) {
+      acc = 2;
+    }
+    if (acc) {
+      if (n == 1) {
+        if (tid == m0 % nthr) s_beads[m0] = pnew1;
+        p_single = pnew1;
+      } else {
+        // the owners install the chain (and its relative positions)
+        QuatProducts qp{};
+        if (rec.rotate) qp = quat_products(rec.q[0], rec.q[1], rec.q[2], rec.q[3]);
+        int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
+        for (; j < m0 + n; j += nthr) {
+          s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
+          if (rec.rotate) {
+            const float4 rl = A.rel[bead_off + j];
+            const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
+            A.rel[bead_off + j] = make_float4(r2.x, r2.y, r2.z, 0.0f);
           }
         }
-        int acc = 0;
-        if (dE < 0.0) {
-          acc = 1;
-        } else if (inf.u5 < exp(-dE * beta)) {
-          acc = 2;
-        }
-        if (acc) {
-          energy += dE;
-          if (acc == 1) ++n_neg; else ++n_boltz;
-          const int m = inf.m;
-          if (inf.rotate) {
-            double* qd = A.quat + 4 * (size_t)(mol_off + m);
-            double out[4];
-            quat_mul(inf.q[0], inf.q[1], inf.q[2], inf.q[3], qd[0], qd[1], qd[2], qd[3], out);
-            qd[0] = out[0];
-            qd[1] = out[1];
-            qd[2] = out[2];
-            qd[3] = out[3];
-          } else {
-            float4 c = s_cent[m];
-            s_cent[m] = make_float4(ctl.nc[0], ctl.nc[1], ctl.nc[2], c.w);
-          }
+      }
+      if (tid == 0) {
+        energy += dE;
+        if (acc == 1) ++n_neg; else ++n_boltz;
+        if (rec.rotate) {
+          double* qd = A.quat + 4 * (size_t)(mol_off + m);
+          double out[4];
+          quat_mul(rec.q[0], rec.q[1], rec.q[2], rec.q[3], qd[0], qd[1], qd[2], qd[3], out);
+          qd[0] = out[0];
+          qd[1] = out[1];
+          qd[2] = out[2];
+          qd[3] = out[3];
         } else {
-          ++n_rej;
+          s_cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
         }
-        ctl.p_acc = acc != 0;
-        ctl.p_m0 = ctl.m0;
-        ctl.p_n = ctl.n_m;
-        ctl.p_rot = ctl.rotate;
-        ctl.p_buf = ctl.buf;
+      }
+    } else if (tid == 0) {
+      ++n_rej;
+    }
+    if (tid == 0 && !skip) {
+      // two evaluations (old and new position) per pair
+      const unsigned long long nn = (unsigned long long)n;
+      if (rec.crowd) {
+        ev_crowd += 2ull * nn * (unsigned long long)(N - n);
+      } else {
+        ev_kh += 2ull * nn * (unsigned long long)(S.n_chain_beads - n);
+        ev_crowd += 2ull * nn * (unsigned long long)(N - S.n_chain_beads);
       }
     }
-    // the next iteration's barrier A orders these writes before their use
+    p_m = m;
+    p_acc = acc != 0;
+    p_rot = rec.rotate;
+    p_n = n;
+    p_b = b;
+    p_nc0 = nc0;
+    p_nc1 = nc1;
+    p_nc2 = nc2;
   }
+  (void)p_n;
   __syncthreads();
 
-  // ---- epilogue: apply the last accepted move, write the instance back
-  {
-    const int pacc = ctl.p_acc, pm0 = ctl.p_m0, pn = ctl.p_n, prot = ctl.p_rot, pb = ctl.p_buf;
-    if (pacc && A.n_steps > 0) {
-      for (int k = tid; k < pn; k += nthr) {
-        s_beads[pm0 + k] = s_tpos[pb * A.lmax + k];
-        if (prot && pn > 1) A.rel[bead_off + pm0 + k] = s_trel[pb * A.lmax + k];
-      }
-    }
-  }
-  __syncthreads();
+  // ---- epilogue: write the instance back
   for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
   for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
   if (tid == 0) {
@@ -568,6 +615,11 @@ struct remc_handle {
   float4* d_centre = nullptr;
   double* d_quat = nullptr;
   int* d_mol_start = nullptr;
+  int* d_mol_role = nullptr;
+  int* d_mrole_off = nullptr;
+  StepRec* d_recs = nullptr;
+  size_t recs_cap = 0;  // records per instance the buffer holds
+  int recs_gen = 0;     // bumped on every reallocation (captured graphs hold the pointer)
   float4* d_tab = nullptr;
   double* d_energy = nullptr;
   int* d_temp_idx = nullptr;
@@ -595,6 +647,7 @@ struct remc_handle {
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = -1;
   uint64_t graph_seed = 0;
+  int graph_recs_gen = -1;
 };
 
 namespace {
@@ -614,7 +667,7 @@ void free_all(remc_handle* h) {
                   h->d_centre,   h->d_quat,      h->d_mol_start,  h->d_tab,        h->d_energy,
                   h->d_temp_idx, h->d_slot_of_temp, h->d_ladder,  h->d_tstep,      h->d_rot_cs,
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
-                  h->d_evals_kh, h->d_evals_crowd,
+                  h->d_evals_kh, h->d_evals_crowd, h->d_mol_role, h->d_mrole_off, h->d_recs,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE};
   for (void* p : ptrs)
@@ -679,8 +732,56 @@ int check_ready(const remc_handle* h) {
   return REMC_OK;
 }
 
-int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0, const uint32_t* ctrl,
-                 const int* inst_list, int n_blocks) {
+// Grow the proposal-record buffer to hold `steps` records per instance.
+int ensure_recs(remc_handle* h, size_t steps) {
+  if (steps <= h->recs_cap) return REMC_OK;
+  if (h->d_recs) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_recs);
+    h->d_recs = nullptr;
+    h->recs_cap = 0;
+  }
+  int rc = dev_alloc(&h->d_recs, steps * (size_t)h->n_inst);
+  if (rc) return rc;
+  h->recs_cap = steps;
+  h->recs_gen++;
+  return REMC_OK;
+}
+
+// Largest number of steps per launch whose records fit the buffer budget.
+size_t max_chunk_steps(const remc_handle* h) {
+  const size_t budget = (size_t)1 << 30;  // 1 GiB of proposal records
+  size_t c = budget / (sizeof(StepRec) * (size_t)h->n_inst);
+  return c < 64 ? 64 : c;
+}
+
+int launch_proposals(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
+                     const uint32_t* ctrl) {
+  ProposalArgs P;
+  P.sys = h->d_sys;
+  P.inst_sys = h->d_inst_sys;
+  P.mol_start = h->d_mol_start;
+  P.mol_role = h->d_mol_role;
+  P.mrole_off = h->d_mrole_off;
+  P.tstep = h->d_tstep;
+  P.rot_cs = h->d_rot_cs;
+  P.recs = h->d_recs;
+  P.ctrl = ctrl;
+  P.step0 = step0;
+  P.seed_lo = (uint32_t)seed;
+  P.seed_hi = (uint32_t)(seed >> 32);
+  P.n_inst = h->n_inst;
+  P.n_steps = n_steps;
+  P.rec_stride = (int)h->recs_cap;
+  const long long total = (long long)h->n_inst * n_steps;
+  const int grid = (int)((total + 255) / 256);
+  proposal_kernel<<<grid, 256, 0, h->stream>>>(P);
+  REMC_CUDA_TRY(cudaGetLastError());
+  return REMC_OK;
+}
+
+int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* inst_list,
+                        int n_blocks) {
   SweepArgs A;
   A.sys = h->d_sys;
   A.inst_sys = h->d_inst_sys;
@@ -691,20 +792,17 @@ int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0, con
   A.quat = h->d_quat;
   A.mol_start = h->d_mol_start;
   A.tab = h->d_tab;
+  A.recs = h->d_recs;
   A.energy = h->d_energy;
   A.temp_idx = h->d_temp_idx;
   A.ladder = h->d_ladder;
-  A.tstep = h->d_tstep;
-  A.rot_cs = h->d_rot_cs;
   A.acc_neg = h->d_acc_neg;
   A.acc_boltz = h->d_acc_boltz;
   A.rej = h->d_rej;
   A.evals_kh = h->d_evals_kh;
   A.evals_crowd = h->d_evals_crowd;
-  A.ctrl = ctrl;
-  A.step0 = step0;
-  A.seed_lo = (uint32_t)seed;
-  A.seed_hi = (uint32_t)(seed >> 32);
+  A.rec_stride = (int)h->recs_cap;
+  A.rec_offset = rec_offset;
   A.n_steps = n_steps;
   A.nmax = h->nmax;
   A.mmax = h->mmax;
@@ -714,6 +812,15 @@ int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0, con
   sweep_kernel<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
   REMC_CUDA_TRY(cudaGetLastError());
   return REMC_OK;
+}
+
+// Proposals then one persistent sweep over all instances, for n_steps steps
+// (the record buffer must already hold n_steps records per instance).
+int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
+                 const uint32_t* ctrl) {
+  int rc = launch_proposals(h, n_steps, seed, step0, ctrl);
+  if (rc) return rc;
+  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst);
 }
 
 }  // namespace
@@ -850,7 +957,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
   }
   // larger systems get more threads per replica
-  h->sweep_threads = h->nmax <= 1024 ? 128 : (h->nmax <= 4096 ? 256 : 512);
+  h->sweep_threads = h->nmax <= 2048 ? 128 : 256;
   // ---- work list of the full-energy kernel (upper-triangle tiles)
   std::vector<TileItem> items;
   std::vector<int> item_off;
@@ -881,6 +988,8 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_centre, h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_quat, 4 * h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_mol_start, h->h_mol_start.size());
+  if (!rc) rc = dev_alloc(&h->d_mol_role, h->h_mol_role.size());
+  if (!rc) rc = dev_alloc(&h->d_mrole_off, h->n_sys);
   if (!rc) rc = dev_alloc(&h->d_tab, (size_t)kNT * kNT);
   if (!rc) rc = dev_alloc(&h->d_energy, h->n_inst);
   if (!rc) rc = dev_alloc(&h->d_temp_idx, h->n_inst);
@@ -910,6 +1019,13 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   up(h->d_inst_sys, h->h_inst_sys.data(), sizeof(int) * h->n_inst);
   up(h->d_inst_list, inst_list.data(), sizeof(int) * h->n_inst);
   up(h->d_mol_start, h->h_mol_start.data(), sizeof(int) * h->h_mol_start.size());
+  up(h->d_mol_role, h->h_mol_role.data(), sizeof(int) * h->h_mol_role.size());
+  std::vector<int> mrole_off(h->n_sys);
+  for (int s2 = 0, off = 0; s2 < h->n_sys; ++s2) {
+    mrole_off[s2] = off;
+    off += h->h_sys[s2].n_mol;
+  }
+  up(h->d_mrole_off, mrole_off.data(), sizeof(int) * h->n_sys);
   up(h->d_items, items.data(), sizeof(TileItem) * items.size());
   up(h->d_item_off, item_off.data(), sizeof(int) * item_off.size());
   if (!rc) {
@@ -1111,21 +1227,38 @@ int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
   int rc = check_ready(h);
   if (rc) return rc;
   if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
-  if (n_steps == 0) return REMC_OK;
-  return launch_sweep(h, n_steps, seed, step0, nullptr, h->d_inst_list, h->n_inst);
+  const size_t chunk_max = max_chunk_steps(h);
+  for (int done = 0; done < n_steps;) {
+    const int chunk = (int)std::min((size_t)(n_steps - done), chunk_max);
+    rc = ensure_recs(h, (size_t)chunk);
+    if (rc) return rc;
+    rc = launch_sweep(h, chunk, seed, step0 + (uint32_t)done, nullptr);
+    if (rc) return rc;
+    done += chunk;
+  }
+  return REMC_OK;
 }
 
 int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
   int rc = check_ready(h);
   if (rc) return rc;
   if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
-  for (int s = 0; s < n_steps; ++s) {
-    for (int g = 0; g < h->n_inst; ++g) {
-      // one single-CTA launch per replica per step; d_inst_list + g names one
-      // instance (instances are independent within a step, so order is free)
-      rc = launch_sweep(h, 1, seed, step0 + (uint32_t)s, nullptr, h->d_inst_list + g, 1);
-      if (rc) return rc;
+  const size_t chunk_max = max_chunk_steps(h);
+  for (int done = 0; done < n_steps;) {
+    const int chunk = (int)std::min((size_t)(n_steps - done), chunk_max);
+    rc = ensure_recs(h, (size_t)chunk);
+    if (rc) return rc;
+    rc = launch_proposals(h, chunk, seed, step0 + (uint32_t)done, nullptr);
+    if (rc) return rc;
+    for (int s = 0; s < chunk; ++s) {
+      for (int g = 0; g < h->n_inst; ++g) {
+        // one single-CTA launch per replica per step; d_inst_list + g names one
+        // instance (instances are independent within a step, so order is free)
+        rc = launch_sweep_kernel(h, 1, s, h->d_inst_list + g, 1);
+        if (rc) return rc;
+      }
     }
+    done += chunk;
   }
   return REMC_OK;
 }
@@ -1239,14 +1372,19 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
   // device control block: step counter, round counter, offset parity
   uint32_t ctrl[4] = {step0, round0, round0 & 1u, 0u};
   REMC_CUDA_TRY(cudaMemcpyAsync(h->d_ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
-  if (!h->graph_exec || h->graph_steps != steps_per_block || h->graph_seed != seed) {
+  if ((size_t)steps_per_block > max_chunk_steps(h))
+    return set_error(REMC_ERR_INVALID, "steps_per_block too large for the record buffer");
+  rc = ensure_recs(h, (size_t)steps_per_block);
+  if (rc) return rc;
+  if (!h->graph_exec || h->graph_steps != steps_per_block || h->graph_seed != seed ||
+      h->graph_recs_gen != h->recs_gen) {
     if (h->graph_exec) {
       cudaGraphExecDestroy(h->graph_exec);
       h->graph_exec = nullptr;
     }
     cudaGraph_t graph;
     REMC_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    rc = launch_sweep(h, steps_per_block, seed, 0, h->d_ctrl, h->d_inst_list, h->n_inst);
+    rc = launch_sweep(h, steps_per_block, seed, 0, h->d_ctrl);
     if (!rc) {
       exchange_kernel<<<h->n_sys, 32, 0, h->stream>>>(
           h->d_sys, h->d_ladder, h->d_energy, h->d_temp_idx, h->d_slot_of_temp, h->d_ex_tests,
@@ -1261,6 +1399,7 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
     if (e != cudaSuccess) return set_error(REMC_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
     h->graph_steps = steps_per_block;
     h->graph_seed = seed;
+    h->graph_recs_gen = h->recs_gen;
   }
   for (int b = 0; b < n_blocks; ++b) REMC_CUDA_TRY(cudaGraphLaunch(h->graph_exec, h->stream));
   return REMC_OK;
