@@ -64,9 +64,18 @@ struct EnergyConsts {
   int crowder_mode;  // 0: A r^-6; 1: A r^-12
 };
 
-// Minimum image d - L*rint(d/L) per axis (CudaFunctions.cu:430-442 uses rintf).
+// Round to nearest, ties to even, on the FMA pipe: adding and subtracting
+// 1.5 * 2^23 leaves the integer part of any |x| < 2^22 in the mantissa and
+// rounds exactly as rintf does (the rounding is the IEEE add's own).
+__device__ __forceinline__ float rint_fma_pipe(float x) {
+  const float kMagic = 12582912.0f;  // 1.5 * 2^23
+  return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
+}
+
+// Minimum image d - L*rint(d/L) per axis (CudaFunctions.cu:430-442 uses rintf);
+// |d/L| stays far below 2^22 for coordinates within a few box lengths.
 __device__ __forceinline__ float min_image(float d, float L, float invL) {
-  return fmaf(-L, rintf(d * invL), d);
+  return fmaf(-L, rint_fma_pipe(d * invL), d);
 }
 
 // Energy (kcal/mol) of one pair of beads of different molecules at squared
@@ -152,6 +161,23 @@ __device__ __forceinline__ void quat_mul(double qw, double qx, double qy, double
                      __dmul_rn(qz, rx));
   out[3] = __dadd_rn(__dsub_rn(__dadd_rn(__dmul_rn(qw, rz), __dmul_rn(qx, ry)), __dmul_rn(qy, rx)),
                      __dmul_rn(qz, rw));
+}
+
+// fmod(x, L) for the wrapped centre of Replica::translate (Replica.cpp:359-361).
+// For x in [0, 3L) the result is x, x - L or x - 2L, and each subtraction is
+// exact (Sterbenz: y/2 <= x <= 2y), so this equals fmodf bit for bit; other
+// inputs (centres placed outside the box) take fmodf itself.
+__device__ __forceinline__ float wrap_box(float x, float L) {
+  if (x >= 0.0f) {
+    if (x < L) return x;
+    const float L2 = 2.0f * L;  // exact
+    if (x < L2) return __fsub_rn(x, L);
+    if (x <= 2.0f * L2) {
+      const float d = __fsub_rn(x, L2);  // exact for L2/2 <= x <= 2 L2
+      if (d < L) return d;
+    }
+  }
+  return fmodf(x, L);
 }
 
 // Translation vector: translate_step * normalise(u2-.5, .5-u3, u4-.5) in FP32.

@@ -73,7 +73,7 @@ struct SysDev {
 // whole sweep, streamed through shared memory by sweep_kernel.
 struct StepRec {
   double q[4];      // step quaternion (rotation)
-  double u5;        // Metropolis uniform
+  double thr;       // Metropolis threshold -log(u)/beta: accept iff dE < thr
   float t[3];       // translation vector
   int m;            // molecule
   int rotate;       // 1 rotation, 0 translation
@@ -89,6 +89,8 @@ struct ProposalArgs {
   const int* mrole_off;  // per system: offset of its roles in mol_role
   const float* tstep;
   const double* rot_cs;
+  const float* ladder;
+  const int* temp_idx;
   StepRec* recs;         // [n_inst][rec_stride]
   const uint32_t* ctrl;
   uint32_t step0;
@@ -117,7 +119,11 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
   r.m = (int)__dmul_rn(u0, (double)S.n_mol);
   const bool crowd = P.mol_role[P.mrole_off[sysid] + r.m] == -1;
   r.rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
-  r.u5 = u5;
+  // u < exp(-beta dE)  <=>  dE < -log(u)/beta  (Replica.cpp:451); u = 0 never
+  // passes the reference's test, so its threshold is -inf
+  const float T = P.ladder[S.inst0 + P.temp_idx[inst]];
+  const double beta = 4184.0 / ((double)8.314472f * (double)T);
+  r.thr = u5 > 0.0 ? -log(u5) / beta : -INFINITY;
   if (r.rotate) {
     step_quaternion(u2, u3, u4, P.rot_cs[2 * inst], P.rot_cs[2 * inst + 1], r.q);
     r.t[0] = r.t[1] = r.t[2] = 0.0f;
@@ -136,7 +142,9 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
 struct SweepArgs {
   const SysDev* sys;
   const int* inst_sys;
-  const int* inst_list;  // CTA -> instance
+  const int* inst_list;  // instances, largest expected cost first
+  int* queue;            // work counter (persistent grid), or null: CTA b runs inst_list[b]
+  int n_list;
   float4* pos;
   float4* rel;
   float4* centre;
@@ -215,7 +223,20 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
 
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
-  const int inst = A.inst_list[blockIdx.x];
+  __shared__ int s_next;
+  for (int it = 0;; ++it) {
+  int idx;
+  if (A.queue) {
+    if (tid == 0) s_next = atomicAdd(A.queue, 1);
+    __syncthreads();
+    idx = s_next;
+    __syncthreads();  // every thread has read s_next before it is rewritten
+    if (idx >= A.n_list) break;
+  } else {
+    if (it > 0) break;
+    idx = blockIdx.x;
+  }
+  const int inst = A.inst_list[idx];
   const int sysid = A.inst_sys[inst];
   const SysDev S = A.sys[sysid];
   const int slot = inst - S.inst0;
@@ -241,8 +262,6 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     cp_async_commit();
     cp_async_wait_all();
   }
-  const float T = A.ladder[S.inst0 + A.temp_idx[inst]];
-  const double beta = 4184.0 / ((double)8.314472f * (double)T);
   double energy = 0.0;
   int n_neg = 0, n_boltz = 0, n_rej = 0;
   unsigned long long ev_kh = 0, ev_crowd = 0;
@@ -284,9 +303,9 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     }
     float nc0 = c0, nc1 = c1, nc2 = c2;
     if (!rec.rotate) {
-      nc0 = fmodf(__fadd_rn(__fadd_rn(c0, rec.t[0]), box), box);
-      nc1 = fmodf(__fadd_rn(__fadd_rn(c1, rec.t[1]), box), box);
-      nc2 = fmodf(__fadd_rn(__fadd_rn(c2, rec.t[2]), box), box);
+      nc0 = wrap_box(__fadd_rn(__fadd_rn(c0, rec.t[0]), box), box);
+      nc1 = wrap_box(__fadd_rn(__fadd_rn(c1, rec.t[1]), box), box);
+      nc2 = wrap_box(__fadd_rn(__fadd_rn(c2, rec.t[2]), box), box);
     }
     // a one-bead rotation moves nothing (its bead sits at the centre): dE = 0
     const bool skip = rec.rotate && n == 1;
@@ -352,12 +371,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     // ---- every thread: the same FP64 sum and the same Metropolis decision
     double dE = 0.0;
     for (int w = 0; w < nwarps; ++w) dE += s_red[b * 32 + w];
-    int acc = 0;
-    if (dE < 0.0) {
-      acc = 1;
-    } else if (rec.u5 < exp(-dE * beta)) {
-      acc = 2;
-    }
+    const int acc = dE < 0.0 ? 1 : (dE < rec.thr ? 2 : 0);
     if (acc) {
       if (n == 1) {
         if (tid == m0 % nthr) s_beads[m0] = pnew1;
@@ -427,6 +441,8 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     A.evals_kh[inst] += ev_kh;
     A.evals_crowd[inst] += ev_crowd;
   }
+  __syncthreads();  // shared memory is reused by the next instance
+  }  // instance loop
 }
 
 // ------------------------------------------------------------------ full E
@@ -635,6 +651,8 @@ struct remc_handle {
   int* d_ex_tests = nullptr;
   int* d_ex_acc = nullptr;
   uint32_t* d_ctrl = nullptr;
+  int* d_queue = nullptr;
+  int sweep_grid = 0;  // resident CTAs of the persistent sweep
   TileItem* d_items = nullptr;
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
@@ -668,6 +686,7 @@ void free_all(remc_handle* h) {
                   h->d_temp_idx, h->d_slot_of_temp, h->d_ladder,  h->d_tstep,      h->d_rot_cs,
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
                   h->d_evals_kh, h->d_evals_crowd, h->d_mol_role, h->d_mrole_off, h->d_recs,
+                  h->d_queue,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE};
   for (void* p : ptrs)
@@ -765,6 +784,8 @@ int launch_proposals(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
   P.mrole_off = h->d_mrole_off;
   P.tstep = h->d_tstep;
   P.rot_cs = h->d_rot_cs;
+  P.ladder = h->d_ladder;
+  P.temp_idx = h->d_temp_idx;
   P.recs = h->d_recs;
   P.ctrl = ctrl;
   P.step0 = step0;
@@ -781,11 +802,17 @@ int launch_proposals(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
 }
 
 int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* inst_list,
-                        int n_blocks) {
+                        int n_blocks, bool persistent) {
   SweepArgs A;
   A.sys = h->d_sys;
   A.inst_sys = h->d_inst_sys;
   A.inst_list = inst_list;
+  A.queue = persistent ? h->d_queue : nullptr;
+  A.n_list = n_blocks;
+  if (persistent) {
+    REMC_CUDA_TRY(cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->stream));
+    n_blocks = std::min(n_blocks, h->sweep_grid);
+  }
   A.pos = h->d_pos;
   A.rel = h->d_rel;
   A.centre = h->d_centre;
@@ -820,7 +847,7 @@ int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
                  const uint32_t* ctrl) {
   int rc = launch_proposals(h, n_steps, seed, step0, ctrl);
   if (rc) return rc;
-  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst);
+  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst, true);
 }
 
 }  // namespace
@@ -958,6 +985,17 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   }
   // larger systems get more threads per replica
   h->sweep_threads = h->nmax <= 2048 ? 128 : 256;
+  {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel, h->sweep_threads,
+                                                      smem);
+    if (e != cudaSuccess || per_sm < 1) {
+      delete h;
+      return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
+                       cudaGetErrorString(e));
+    }
+    h->sweep_grid = per_sm * h->num_sms;
+  }
   // ---- work list of the full-energy kernel (upper-triangle tiles)
   std::vector<TileItem> items;
   std::vector<int> item_off;
@@ -976,9 +1014,21 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (e != cudaSuccess) rc = set_error(REMC_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
   std::vector<int> inst_list(h->n_inst);
   for (int g = 0; g < h->n_inst; ++g) inst_list[g] = g;
-  // largest systems first: the block scheduler starts them earliest
+  // largest expected cost first (longest-processing-time order for the work
+  // queue): expected pair evaluations per step = sum_m n_m (N - n_m) / M
+  std::vector<double> sys_cost(h->n_sys, 0.0);
+  for (int s2 = 0; s2 < h->n_sys; ++s2) {
+    const SysDev& S = h->h_sys[s2];
+    const int* ms = &h->h_mol_start[S.mstart_off];
+    double c = 0.0;
+    for (int m = 0; m < S.n_mol; ++m) {
+      const double n = ms[m + 1] - ms[m];
+      c += n * (S.n_beads - n);
+    }
+    sys_cost[s2] = c / S.n_mol + S.n_beads;  // + per-step bookkeeping
+  }
   std::stable_sort(inst_list.begin(), inst_list.end(), [&](int a, int b) {
-    return h->h_sys[h->h_inst_sys[a]].n_beads > h->h_sys[h->h_inst_sys[b]].n_beads;
+    return sys_cost[h->h_inst_sys[a]] > sys_cost[h->h_inst_sys[b]];
   });
   if (!rc) rc = dev_alloc(&h->d_sys, h->h_sys.size());
   if (!rc) rc = dev_alloc(&h->d_inst_sys, h->n_inst);
@@ -1005,6 +1055,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_ex_tests, h->n_sys);
   if (!rc) rc = dev_alloc(&h->d_ex_acc, h->n_sys);
   if (!rc) rc = dev_alloc(&h->d_ctrl, 4);
+  if (!rc) rc = dev_alloc(&h->d_queue, 1);
   if (!rc) rc = dev_alloc(&h->d_items, items.size());
   if (!rc) rc = dev_alloc(&h->d_item_off, item_off.size());
   if (!rc) rc = dev_alloc(&h->d_scratch, items.size());
@@ -1254,7 +1305,7 @@ int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0)
       for (int g = 0; g < h->n_inst; ++g) {
         // one single-CTA launch per replica per step; d_inst_list + g names one
         // instance (instances are independent within a step, so order is free)
-        rc = launch_sweep_kernel(h, 1, s, h->d_inst_list + g, 1);
+        rc = launch_sweep_kernel(h, 1, s, h->d_inst_list + g, 1, false);
         if (rc) return rc;
       }
     }
