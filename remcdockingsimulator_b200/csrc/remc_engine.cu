@@ -35,12 +35,19 @@
 #include <vector>
 
 #include "remc_device.cuh"
+#include "remc_internal.h"
 
 using namespace remc;
 
 namespace {
 
 thread_local std::string g_last_error;
+
+}  // namespace
+
+void remc::record_error(const char* message) { g_last_error = message ? message : ""; }
+
+namespace {
 
 int set_error(int code, const char* fmt, ...) {
   char buf[512];
