@@ -93,6 +93,30 @@ void CUDA_freeBoxDimension(void);
 void bindLJTexture(float* ljp);
 void unbindLJTexture(void);
 
+/* Allocation-free variant of CUDA_EonDevice. No counterpart in the reference:
+ * the reference's CUDA_EonDevice allocates and frees its partial sums on every
+ * call. This entry point allocates nothing, for callers that cannot call
+ * cudaMalloc: hosts whose device memory is owned by another allocator (a
+ * framework's caching arena that has reserved the GPU), and loops that cannot
+ * afford cudaMalloc/cudaFree's implicit device synchronisation on every Monte
+ * Carlo step. The caller passes device inputs (same layout as CUDA_EonDevice)
+ * and a device pointer for the result (one double, kcal/mol); the work is
+ * ordered on `stream` and the call does not wait for it. The partial sums live
+ * in one fixed device array of REMC_NOALLOC_MAX_ITEMS doubles (256 KiB) that
+ * every GPU loading this library holds until the process exits, so
+ * datasetSize is limited to REMC_NOALLOC_MAX_BEADS beads; larger sizes return
+ * REMC_ERR_INVALID with a message. The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture on that device. All calls share the array and each call
+ * overwrites every partial it reads, so nothing needs clearing between calls;
+ * calls that overlap on the GPU (different streams, or different host threads
+ * on one device) race on it. Returns REMC_OK or a negative REMC_ERR_* code. */
+#define REMC_NOALLOC_MAX_ITEMS 32768
+#define REMC_NOALLOC_MAX_BEADS 32640
+int CUDA_EonDevice_noalloc(const float4* residuePositions, const float4* residueMeta,
+                           const float* LJPotentials, int datasetSize, double* d_result,
+                           cudaStream_t stream);
+
 /* Energy-model constants used by the calls above (default: the reference's
  * compile-time values, remc_default_params). No reference counterpart. */
 int remc_reference_abi_set_params(const remc_params* params);

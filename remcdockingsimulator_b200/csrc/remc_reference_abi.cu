@@ -229,6 +229,18 @@ double* device_scratch(size_t n) {
   return g_scratch[dev];
 }
 
+// ---- allocation-free energy (CUDA_EonDevice_noalloc)
+// Fixed scratch for the per-item partials: a file-scope device array, so the
+// entry point never allocates. Every GPU that loads this library holds it
+// (256 KiB) until the process exits. REMC_NOALLOC_MAX_ITEMS items of 128 x 128
+// beads cover up to 255 tiles, i.e. 32640 beads.
+constexpr int kNoAllocMaxItems = REMC_NOALLOC_MAX_ITEMS;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxItems];
+
+// Device address of g_noalloc_scratch, looked up once per device (the host
+// name of a __device__ array is only a host-side stand-in).
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
 bool energy_args_ok(const float4* pos, const float4* meta, const float* table, int P) {
   if (!pos || !meta) {
     set_status(REMC_ERR_INVALID, "null position or metadata pointer");
@@ -459,6 +471,66 @@ void unbindLJTexture(void) {
   std::lock_guard<std::mutex> lock(g_mutex);
   g_bound_table = nullptr;
   g_status = REMC_OK;
+}
+
+int CUDA_EonDevice_noalloc(const float4* pos, const float4* meta, const float* LJPotentials,
+                           int datasetSize, double* d_result, cudaStream_t stream) {
+  const float* table = LJPotentials ? LJPotentials : g_bound_table;
+  if (!d_result) {
+    set_status(REMC_ERR_INVALID, "null result pointer");
+    return REMC_ERR_INVALID;
+  }
+  if (!energy_args_ok(pos, meta, table, datasetSize)) return g_status;
+  const int T = (datasetSize + kRefTile - 1) / kRefTile;
+  const long long n = (long long)T * (T + 1) / 2;
+  if (n > kNoAllocMaxItems) {
+    char buf[160];
+    snprintf(buf, sizeof(buf),
+             "datasetSize %d exceeds the allocation-free limit of %d beads (%d tile pairs)",
+             datasetSize, REMC_NOALLOC_MAX_BEADS, kNoAllocMaxItems);
+    set_status(REMC_ERR_INVALID, buf);
+    return REMC_ERR_INVALID;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    set_status(REMC_ERR_CUDA, "cudaGetDevice", e);
+    return REMC_ERR_CUDA;
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      // once per device, with that device current
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        set_status(REMC_ERR_CUDA, "cudaGetSymbolAddress(scratch)", e);
+        return REMC_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  // every item writes its partial before the sum reads it: no clearing needed
+  const RefConsts C = make_consts();
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(T * T, sms * 8);
+  ref_energy_tiles<<<grid, kRefTile, 0, stream>>>(pos, meta, table, datasetSize, T, scratch, C);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_status(REMC_ERR_CUDA, "energy kernel launch", e);
+    return REMC_ERR_CUDA;
+  }
+  ref_energy_sum<<<1, 256, 0, stream>>>(scratch, (int)n, d_result, nullptr, 0, 1.0f);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_status(REMC_ERR_CUDA, "energy sum launch", e);
+    return REMC_ERR_CUDA;
+  }
+  set_status(REMC_OK, "");
+  return REMC_OK;
 }
 
 }  // extern "C"

@@ -37,6 +37,7 @@ def abi() -> C.CDLL:
             "bindLJTexture": (None, [P]),
             "unbindLJTexture": (None, []),
             "remc_reference_abi_status": (C.c_int, []),
+            "CUDA_EonDevice_noalloc": (C.c_int, [P, P, P, C.c_int, P, P]),
             "CUDA_memcpy_to_device": (C.c_int, [P, P, C.c_int]),
             "CUDA_memcpy_to_host": (C.c_int, [P, P, C.c_int]),
         }
