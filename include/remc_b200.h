@@ -136,6 +136,42 @@ int remc_reset_counters(remc_handle* h);
  * pairs involving a crowder. A dE pair counts twice (old and new position). */
 int remc_get_pair_evaluations(remc_handle* h, uint64_t* residue_pairs, uint64_t* crowder_pairs);
 
+/* Sampling (Replica::sample, Replica.cpp:1717-1780, driven as in
+ * MCthreadableFunction, main.cpp:975-989): inside every sweep, after each
+ * chunk of `sample_every` steps, a replica is sampled if the chunk's label
+ * (sweep start step + chunk start) is >= sample_after. It counts as bound if
+ * its potential, plus the chain-chain pair energy when crowders are present
+ * (the reference's sum), is below bound_threshold (-1.1844 kcal/mol in the
+ * reference, definitions.h:84). Bound samples append a record and one pose per
+ * molecule to device buffers of max_records / max_poses entries (0: count
+ * only); records that do not fit are counted as dropped. sample_every = 0
+ * turns sampling off. Chains must precede crowders in every system. */
+typedef struct {
+  int inst;
+  uint32_t label;
+  double e_noncrowder;  /* the value compared with the threshold */
+  double e_total;       /* potential */
+  float temperature;
+  int n_mol;
+  int pose_offset;      /* first pose of this record in the pose array */
+} remc_sample;
+typedef struct {
+  double q[4];          /* rotation quaternion w, x, y, z */
+  float centre[3];
+} remc_sample_pose;
+int remc_set_sampling(remc_handle* h, int sample_every, uint32_t sample_after,
+                      double bound_threshold, int max_records, int max_poses);
+/* Per-instance samples taken and bound samples since the last counter reset. */
+int remc_get_sample_counters(remc_handle* h, int* samples, int* bound);
+/* Copy out the records and poses written since the last call and clear the
+ * buffers. n_dropped receives the records that did not fit. */
+int remc_read_samples(remc_handle* h, remc_sample* records, int max_records,
+                      remc_sample_pose* poses, int max_poses, int* n_records, int* n_poses,
+                      int* n_dropped);
+/* Chain-chain part of each instance's energy (sum of E(Molecule*,Molecule*)
+ * over chain pairs, Replica.cpp:793-828), tracked with the running energy. */
+int remc_get_noncrowder_energies(remc_handle* h, double* out);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after the engine's. */
 int remc_get_stream(remc_handle* h, void** stream);

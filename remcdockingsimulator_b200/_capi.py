@@ -35,6 +35,16 @@ class Params(C.Structure):
                 ("crowder_eps", C.c_float)]
 
 
+class SampleRecord(C.Structure):
+    _fields_ = [("inst", C.c_int), ("label", C.c_uint32), ("e_noncrowder", C.c_double),
+                ("e_total", C.c_double), ("temperature", C.c_float), ("n_mol", C.c_int),
+                ("pose_offset", C.c_int)]
+
+
+class SamplePose(C.Structure):
+    _fields_ = [("q", C.c_double * 4), ("centre", C.c_float * 3)]
+
+
 class SystemDesc(C.Structure):
     _fields_ = [("n_beads", C.c_int), ("n_mol", C.c_int), ("n_replicas", C.c_int),
                 ("mol_start", C.POINTER(C.c_int)), ("mol_role", C.POINTER(C.c_int)),
@@ -71,6 +81,11 @@ _SIGS = {
     "remc_sync": (C.c_int, [P]),
     "remc_get_pair_evaluations": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "remc_get_stream": (C.c_int, [P, C.POINTER(C.c_void_p)]),
+    "remc_set_sampling": (C.c_int, [P, C.c_int, C.c_uint32, C.c_double, C.c_int, C.c_int]),
+    "remc_get_sample_counters": (C.c_int, [P, PI, PI]),
+    "remc_read_samples": (C.c_int, [P, C.POINTER(SampleRecord), C.c_int, C.POINTER(SamplePose),
+                                    C.c_int, PI, PI, PI]),
+    "remc_get_noncrowder_energies": (C.c_int, [P, PD]),
     "remc_num_instances": (C.c_int, [P]),
     "remc_last_error_string": (C.c_char_p, []),
 }

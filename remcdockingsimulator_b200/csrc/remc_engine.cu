@@ -146,6 +146,24 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
   P.recs[(size_t)inst * P.rec_stride + s] = r;
 }
 
+// A bound conformation recorded by Replica::sample (Replica.cpp:1717-1780):
+// header + one pose (rotation quaternion, centre) per molecule.
+struct SampleHeader {
+  int inst;
+  uint32_t label;     // step label (start of the sampling chunk, main.cpp:983-987)
+  double e_nc;        // potential + chain-chain pair energy (the sample() sum)
+  double e;           // potential
+  float temperature;
+  int n_mol;
+  uint32_t pose_offset;
+  int pad;
+};
+struct SamplePose {
+  double q[4];
+  float c[3];
+  float pad;
+};
+
 struct SweepArgs {
   const SysDev* sys;
   const int* inst_sys;
@@ -160,8 +178,21 @@ struct SweepArgs {
   const float4* tab;
   const StepRec* recs;   // [n_inst][rec_stride]
   double* energy;
+  double* ecc;           // chain-chain part of the energy (sample() sum)
   const int* temp_idx;
   const float* ladder;
+  // sampling (Replica::sample): every `sample_every` steps, labels from step0
+  int sample_every;
+  uint32_t sample_after;
+  double bound_thr;
+  const uint32_t* ctrl;
+  uint32_t step0;
+  int* n_samples;
+  int* n_bound;
+  SampleHeader* sample_out;
+  SamplePose* pose_out;
+  unsigned* sample_cursor;  // [0] records, [1] poses, [2] dropped
+  unsigned sample_cap, pose_cap;
   int* acc_neg;          // accepted with dE < 0
   int* acc_boltz;        // accepted by the Boltzmann test
   int* rej;
@@ -170,6 +201,7 @@ struct SweepArgs {
   int rec_stride, rec_offset;       // records of step s at rec_offset + s
   int n_steps;
   int nmax, mmax, lmax;  // shared-memory capacities
+  int mol_in_smem;       // centres and molecule starts resident in shared memory
   EnergyConsts K;
 };
 
@@ -184,16 +216,18 @@ struct SweepSmem {
     off += (bytes + 15) & ~size_t(15);
     return o;
   }
-  static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax) {
+  // mol_in_smem = 0: molecule centres and starts stay in global memory (the
+  // largest systems), everything else as usual
+  static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax, int mol_in_smem) {
     SweepSmem s;
     size_t off = 0;
     s.tab = take(off, sizeof(float4) * kNT * kNT);
     s.beads = take(off, sizeof(float4) * nmax);
-    s.centres = take(off, sizeof(float4) * mmax);
+    s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
-    s.mstart = take(off, sizeof(int) * (mmax + 1));
+    s.mstart = take(off, mol_in_smem ? sizeof(int) * (mmax + 1) : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
-    s.red = take(off, sizeof(double) * 2 * 32);
+    s.red = take(off, sizeof(double) * 2 * 2 * 32);
     s.total = off;
     return s;
   }
@@ -219,7 +253,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // costs two (trial positions are built by the owners of the chain's beads).
 __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax);
+  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
   float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
@@ -257,8 +291,15 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
   for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
-  for (int i = tid; i < M; i += nthr) s_cent[i] = A.centre[mol_off + i];
-  for (int i = tid; i <= M; i += nthr) s_mstart[i] = A.mol_start[S.mstart_off + i];
+  // molecule centres and starts: shared memory, or global memory for the
+  // largest systems (thread 0 writes a centre; others read it only after a
+  // later barrier, which orders global memory within the CTA as well)
+  float4* cent = A.mol_in_smem ? s_cent : A.centre + mol_off;
+  const int* mst = A.mol_in_smem ? s_mstart : A.mol_start + S.mstart_off;
+  if (A.mol_in_smem) {
+    for (int i = tid; i < M; i += nthr) s_cent[i] = A.centre[mol_off + i];
+    for (int i = tid; i <= M; i += nthr) s_mstart[i] = A.mol_start[S.mstart_off + i];
+  }
   {
     // first ring fill: records of steps 0..min(kRing, n_steps)-1, 16 B per copy
     const int nrec = min(kRing, n_steps);
@@ -269,10 +310,13 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     cp_async_commit();
     cp_async_wait_all();
   }
-  double energy = 0.0;
-  int n_neg = 0, n_boltz = 0, n_rej = 0;
+  // every thread keeps the running energies (all see the same dE and decision)
+  double energy = A.energy[inst], ecc = A.ecc[inst];
+  int n_neg = 0, n_boltz = 0, n_rej = 0, n_samp = 0, n_bnd = 0;
   unsigned long long ev_kh = 0, ev_crowd = 0;
-  if (tid == 0) energy = A.energy[inst];
+  const int ncb = S.n_chain_beads;  // beads [0, ncb) belong to chains
+  const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
+  __shared__ long long s_pose_slot;
   __syncthreads();
 
   // previous step, known to every thread
@@ -293,7 +337,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     }
     const StepRec rec = s_ring[s & (kRing - 1)];
     const int m = rec.m;
-    const int m0 = s_mstart[m], n = s_mstart[m + 1] - m0;
+    const int m0 = mst[m], n = mst[m + 1] - m0;
     const int b = s & 1;
     const bool same = (m == p_m) && p_acc;  // moved (and accepted) last step
     // centre of m: the one this step's thread computed last step if m moved then
@@ -303,7 +347,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
       c1 = p_nc1;
       c2 = p_nc2;
     } else {
-      const float4 c = s_cent[m];
+      const float4 c = cent[m];
       c0 = c.x;
       c1 = c.y;
       c2 = c.z;
@@ -341,8 +385,10 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
       __syncthreads();  // trial positions and the previous chain update visible
     }
 
-    // ---- dE over beads j outside the molecule (thread t owns j = t mod T)
-    double dacc = 0.0;
+    // ---- dE over beads j outside the molecule (thread t owns j = t mod T);
+    // for a chain, the part from other chains' beads (j < ncb) is kept apart:
+    // it is the change of the chain-chain energy sample() adds
+    double dacc = 0.0, dcc = 0.0;
     if (!skip) {
       for (int k = 0; k < n; ++k) {
         float4 pold, pnew;
@@ -356,8 +402,18 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
         const int ta = bead_type(pold.w);
         const bool a_crowd = ta >= kNumAmino;
         const float4* trow = s_tab + ta * kNT;
-        float acc = 0.0f;
-        for (int j = tid; j < N; j += nthr) {
+        float acc_c = 0.0f, acc_o = 0.0f;
+        int j = tid;
+        for (; j < ncb; j += nthr) {
+          if (j >= m0 && j < m0 + n) continue;
+          const float4 pj = s_beads[j];
+          const int tb = bead_type(pj.w);
+          const float4 Tj = trow[tb];
+          const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, a_crowd, A.K);
+          const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, a_crowd, A.K);
+          acc_c += en - eo;
+        }
+        for (; j < N; j += nthr) {
           if (j >= m0 && j < m0 + n) continue;
           const float4 pj = s_beads[j];
           const int tb = bead_type(pj.w);
@@ -365,21 +421,35 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
           const bool crowd = a_crowd || tb >= kNumAmino;
           const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
           const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
-          acc += en - eo;
+          acc_o += en - eo;
         }
-        dacc += (double)acc;
+        if (a_crowd) {
+          dacc += (double)acc_c + (double)acc_o;
+        } else {
+          dcc += (double)acc_c;
+          dacc += (double)acc_o;
+        }
       }
     }
     dacc = warp_sum(dacc);
-    if (lane == 0) s_red[b * 32 + warp] = dacc;
+    if (!rec.crowd) dcc = warp_sum(dcc);
+    if (lane == 0) {
+      s_red[b * 64 + warp] = dacc;
+      s_red[b * 64 + 32 + warp] = dcc;
+    }
     if ((s & 31) == 31) cp_async_wait_all();  // next ring half has landed
     __syncthreads();  // R: partial sums (and the prefetched records) visible
 
-    // ---- every thread: the same FP64 sum and the same Metropolis decision
-    double dE = 0.0;
-    for (int w = 0; w < nwarps; ++w) dE += s_red[b * 32 + w];
+    // ---- every thread: the same FP64 sums and the same Metropolis decision
+    double dE_cc = 0.0, dE = 0.0;
+    if (!rec.crowd)
+      for (int w = 0; w < nwarps; ++w) dE_cc += s_red[b * 64 + 32 + w];
+    for (int w = 0; w < nwarps; ++w) dE += s_red[b * 64 + w];
+    dE += dE_cc;
     const int acc = dE < 0.0 ? 1 : (dE < rec.thr ? 2 : 0);
     if (acc) {
+      energy += dE;
+      ecc += dE_cc;
       if (n == 1) {
         if (tid == m0 % nthr) s_beads[m0] = pnew1;
         p_single = pnew1;
@@ -398,7 +468,6 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
         }
       }
       if (tid == 0) {
-        energy += dE;
         if (acc == 1) ++n_neg; else ++n_boltz;
         if (rec.rotate) {
           double* qd = A.quat + 4 * (size_t)(mol_off + m);
@@ -409,7 +478,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
           qd[2] = out[2];
           qd[3] = out[3];
         } else {
-          s_cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
+          cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
         }
       }
     } else if (tid == 0) {
@@ -423,6 +492,61 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
       } else {
         ev_kh += 2ull * nn * (unsigned long long)(S.n_chain_beads - n);
         ev_crowd += 2ull * nn * (unsigned long long)(N - S.n_chain_beads);
+      }
+    }
+    // ---- Replica::sample at the end of every sampling chunk (main.cpp:975-989):
+    // bound if potential (+ chain-chain energy when crowders exist) < threshold
+    if (A.sample_every > 0 && ((s + 1) % A.sample_every) == 0) {
+      const uint32_t label = step0 + (uint32_t)(s + 1 - A.sample_every);
+      if (label >= A.sample_after) {
+        const double enc = (ncb < N) ? energy + ecc : energy;
+        const bool bound = enc < A.bound_thr;
+        if (tid == 0) {
+          ++n_samp;
+          n_bnd += bound ? 1 : 0;
+        }
+        if (bound && A.sample_out) {
+          __syncthreads();  // this step's centre / rotation writes visible
+          if (tid == 0) {
+            const unsigned r = atomicAdd(&A.sample_cursor[0], 1u);
+            const unsigned p0 = atomicAdd(&A.sample_cursor[1], (unsigned)M);
+            if (r < A.sample_cap && (unsigned long long)p0 + M <= A.pose_cap) {
+              SampleHeader hd;
+              hd.inst = inst;
+              hd.label = label;
+              hd.e_nc = enc;
+              hd.e = energy;
+              hd.temperature = A.ladder[S.inst0 + A.temp_idx[inst]];
+              hd.n_mol = M;
+              hd.pose_offset = p0;
+              hd.pad = 0;
+              A.sample_out[r] = hd;
+              s_pose_slot = p0;
+            } else {
+              atomicAdd(&A.sample_cursor[2], 1u);
+              s_pose_slot = -1;
+            }
+          }
+          __syncthreads();
+          const long long p0 = s_pose_slot;
+          if (p0 >= 0) {
+            for (int i = tid; i < M; i += nthr) {
+              const double* qd = A.quat + 4 * (size_t)(mol_off + i);
+              const float4 c = cent[i];
+              SamplePose ps;
+              ps.q[0] = qd[0];
+              ps.q[1] = qd[1];
+              ps.q[2] = qd[2];
+              ps.q[3] = qd[3];
+              ps.c[0] = c.x;
+              ps.c[1] = c.y;
+              ps.c[2] = c.z;
+              ps.pad = 0.0f;
+              A.pose_out[p0 + i] = ps;
+            }
+          }
+          __syncthreads();  // poses read before the next step moves anything
+        }
       }
     }
     p_m = m;
@@ -439,9 +563,13 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
 
   // ---- epilogue: write the instance back
   for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
-  for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
+  if (A.mol_in_smem)
+    for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
   if (tid == 0) {
     A.energy[inst] = energy;
+    A.ecc[inst] = ecc;
+    A.n_samples[inst] += n_samp;
+    A.n_bound[inst] += n_bnd;
     A.acc_neg[inst] += n_neg;
     A.acc_boltz[inst] += n_boltz;
     A.rej[inst] += n_rej;
@@ -463,10 +591,11 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
     const TileItem* __restrict__ items, int n_items, double* __restrict__ scratch,
-    EnergyConsts K) {
+    double* __restrict__ scratch_cc, EnergyConsts K) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
   __shared__ double s_red[kTile / 32];
+  __shared__ double s_red_cc[kTile / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -481,44 +610,65 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     if (tid < jn) s_j[tid] = pos[base + j0 + tid];
     __syncthreads();
     const int i = W.ti * kTile + tid;
-    double dsum = 0.0;
+    double dsum = 0.0, dcc = 0.0;
     if (i < N) {
       const float4 pi = pos[base + i];
       const int ta = bead_type(pi.w), mi = bead_mol(pi.w);
       const bool a_crowd = ta >= kNumAmino;
       const int jstart = (W.ti == W.tj) ? tid + 1 : 0;
-      float acc = 0.0f;
+      float acc = 0.0f, acc_cc = 0.0f;  // all pairs; chain-chain pairs
       for (int jj = jstart; jj < jn; ++jj) {
         const float4 pj = s_j[jj];
         if (bead_mol(pj.w) == mi) continue;
         const int tb = bead_type(pj.w);
         const float4 Tij = s_tab[tb * kNT + ta];
-        acc += pair_energy_r2(pair_r2(pi, pj, box, invbox), Tij, a_crowd || tb >= kNumAmino, K);
+        const bool crowd = a_crowd || tb >= kNumAmino;
+        const float e = pair_energy_r2(pair_r2(pi, pj, box, invbox), Tij, crowd, K);
+        acc += e;
+        if (!crowd) acc_cc += e;
       }
       dsum = (double)acc;
+      dcc = (double)acc_cc;
     }
     dsum = warp_sum(dsum);
-    if (lane == 0) s_red[warp] = dsum;
+    dcc = warp_sum(dcc);
+    if (lane == 0) {
+      s_red[warp] = dsum;
+      s_red_cc[warp] = dcc;
+    }
     __syncthreads();
     if (tid == 0) {
-      double v = 0.0;
-      for (int w = 0; w < kTile / 32; ++w) v += s_red[w];
+      double v = 0.0, c = 0.0;
+      for (int w = 0; w < kTile / 32; ++w) {
+        v += s_red[w];
+        c += s_red_cc[w];
+      }
       scratch[it] = v;
+      scratch_cc[it] = c;
     }
   }
 }
 
 // Per-instance fixed-order sum of the tile partials.
 __global__ void energy_reduce_kernel(const int* __restrict__ item_off, int n_inst,
-                                     const double* __restrict__ scratch, double* __restrict__ energy) {
+                                     const double* __restrict__ scratch,
+                                     const double* __restrict__ scratch_cc,
+                                     double* __restrict__ energy, double* __restrict__ ecc) {
   const int inst = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (inst >= n_inst) return;
   const int a = item_off[inst], b = item_off[inst + 1];
-  double v = 0.0;
-  for (int i = a + lane; i < b; i += 32) v += scratch[i];
+  double v = 0.0, c = 0.0;
+  for (int i = a + lane; i < b; i += 32) {
+    v += scratch[i];
+    c += scratch_cc[i];
+  }
   v = warp_sum(v);
-  if (lane == 0) energy[inst] = v;
+  c = warp_sum(c);
+  if (lane == 0) {
+    energy[inst] = v;
+    ecc[inst] = c;
+  }
 }
 
 // ------------------------------------------------------------------ exchange
@@ -660,9 +810,22 @@ struct remc_handle {
   uint32_t* d_ctrl = nullptr;
   int* d_queue = nullptr;
   int sweep_grid = 0;  // resident CTAs of the persistent sweep
+  int mol_in_smem = 1; // molecule centres/starts in shared memory (else global)
   TileItem* d_items = nullptr;
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
+  double* d_scratch_cc = nullptr;
+  double* d_ecc = nullptr;
+  int* d_n_samples = nullptr;
+  int* d_n_bound = nullptr;
+  SampleHeader* d_sample_out = nullptr;
+  SamplePose* d_pose_out = nullptr;
+  unsigned* d_sample_cursor = nullptr;
+  unsigned sample_cap = 0, pose_cap = 0;
+  int sample_every = 0;
+  uint32_t sample_after = 0;
+  double bound_thr = -1.1844;
+  int sample_gen = 0;  // bumped when sampling changes (captured graphs hold it)
   int n_items = 0;
   float4* d_newpos = nullptr;
   double* d_dE = nullptr;
@@ -673,6 +836,7 @@ struct remc_handle {
   int graph_steps = -1;
   uint64_t graph_seed = 0;
   int graph_recs_gen = -1;
+  int graph_sample_gen = -1;
 };
 
 namespace {
@@ -693,7 +857,8 @@ void free_all(remc_handle* h) {
                   h->d_temp_idx, h->d_slot_of_temp, h->d_ladder,  h->d_tstep,      h->d_rot_cs,
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
                   h->d_evals_kh, h->d_evals_crowd, h->d_mol_role, h->d_mrole_off, h->d_recs,
-                  h->d_queue,
+                  h->d_queue,      h->d_scratch_cc, h->d_ecc,     h->d_n_samples,  h->d_n_bound,
+                  h->d_sample_out, h->d_pose_out, h->d_sample_cursor,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE};
   for (void* p : ptrs)
@@ -809,7 +974,7 @@ int launch_proposals(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
 }
 
 int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* inst_list,
-                        int n_blocks, bool persistent) {
+                        int n_blocks, bool persistent, uint32_t step0, const uint32_t* ctrl) {
   SweepArgs A;
   A.sys = h->d_sys;
   A.inst_sys = h->d_inst_sys;
@@ -828,8 +993,21 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.tab = h->d_tab;
   A.recs = h->d_recs;
   A.energy = h->d_energy;
+  A.ecc = h->d_ecc;
   A.temp_idx = h->d_temp_idx;
   A.ladder = h->d_ladder;
+  A.sample_every = h->sample_every;
+  A.sample_after = h->sample_after;
+  A.bound_thr = h->bound_thr;
+  A.ctrl = ctrl;
+  A.step0 = step0;
+  A.n_samples = h->d_n_samples;
+  A.n_bound = h->d_n_bound;
+  A.sample_out = h->d_sample_out;
+  A.pose_out = h->d_pose_out;
+  A.sample_cursor = h->d_sample_cursor;
+  A.sample_cap = h->sample_cap;
+  A.pose_cap = h->pose_cap;
   A.acc_neg = h->d_acc_neg;
   A.acc_boltz = h->d_acc_boltz;
   A.rej = h->d_rej;
@@ -840,9 +1018,10 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.n_steps = n_steps;
   A.nmax = h->nmax;
   A.mmax = h->mmax;
+  A.mol_in_smem = h->mol_in_smem;
   A.lmax = h->lmax;
   A.K = consts_of(h);
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax).total;
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem).total;
   sweep_kernel<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
   REMC_CUDA_TRY(cudaGetLastError());
   return REMC_OK;
@@ -854,7 +1033,7 @@ int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
                  const uint32_t* ctrl) {
   int rc = launch_proposals(h, n_steps, seed, step0, ctrl);
   if (rc) return rc;
-  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst, true);
+  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst, true, step0, ctrl);
 }
 
 }  // namespace
@@ -906,6 +1085,14 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
       return set_error(REMC_ERR_INVALID, "system %d: mol_start must run 0..n_beads", s);
     }
     int lmax = 0;
+    for (int m = 1; m < d.n_mol; ++m) {
+      if (d.mol_role[m] == 0 && d.mol_role[m - 1] == -1) {
+        delete h;
+        return set_error(REMC_ERR_INVALID,
+                         "system %d: chains must precede crowders (the reference's files "
+                         "section precedes its crowders section)", s);
+      }
+    }
     for (int m = 0; m < d.n_mol; ++m) {
       int n = d.mol_start[m + 1] - d.mol_start[m];
       if (n <= 0) {
@@ -963,7 +1150,6 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   h->n_inst = inst_cursor;
   h->total_beads = bead_cursor;
   h->total_mols = mol_cursor;
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax).total;
   cudaError_t e = cudaGetDevice(&h->device);
   if (e != cudaSuccess) {
     delete h;
@@ -979,6 +1165,11 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     return set_error(REMC_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
   }
   const int max_dyn = max_smem - (int)fattr.sharedSizeBytes;
+  size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, 1).total;
+  if (smem > (size_t)max_dyn) {
+    h->mol_in_smem = 0;
+    smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, 0).total;
+  }
   if (smem > (size_t)max_dyn) {
     delete h;
     return set_error(REMC_ERR_INVALID,
@@ -1066,6 +1257,11 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_items, items.size());
   if (!rc) rc = dev_alloc(&h->d_item_off, item_off.size());
   if (!rc) rc = dev_alloc(&h->d_scratch, items.size());
+  if (!rc) rc = dev_alloc(&h->d_scratch_cc, items.size());
+  if (!rc) rc = dev_alloc(&h->d_ecc, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_n_samples, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_n_bound, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_sample_cursor, 4);
   if (!rc) rc = dev_alloc(&h->d_newpos, h->lmax);
   if (!rc) rc = dev_alloc(&h->d_dE, 1);
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -1095,6 +1291,10 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     cudaMemsetAsync(h->d_ex_tests, 0, sizeof(int) * h->n_sys, h->stream);
     cudaMemsetAsync(h->d_ex_acc, 0, sizeof(int) * h->n_sys, h->stream);
     cudaMemsetAsync(h->d_energy, 0, sizeof(double) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_ecc, 0, sizeof(double) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_n_samples, 0, sizeof(int) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_n_bound, 0, sizeof(int) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_sample_cursor, 0, sizeof(unsigned) * 4, h->stream);
     cudaMemsetAsync(h->d_ctrl, 0, sizeof(uint32_t) * 4, h->stream);
     e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) rc = set_error(REMC_ERR_CUDA, "create sync: %s", cudaGetErrorString(e));
@@ -1260,10 +1460,10 @@ int remc_energy_full(remc_handle* h, double* out) {
   int grid = std::min(h->n_items, h->num_sms * 8);
   energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
                                                    h->d_items, h->n_items, h->d_scratch,
-                                                   consts_of(h));
+                                                   h->d_scratch_cc, consts_of(h));
   REMC_CUDA_TRY(cudaGetLastError());
-  energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(h->d_item_off, h->n_inst,
-                                                                  h->d_scratch, h->d_energy);
+  energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(
+      h->d_item_off, h->n_inst, h->d_scratch, h->d_scratch_cc, h->d_energy, h->d_ecc);
   REMC_CUDA_TRY(cudaGetLastError());
   if (out) {
     REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_energy, sizeof(double) * h->n_inst,
@@ -1312,7 +1512,8 @@ int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0)
       for (int g = 0; g < h->n_inst; ++g) {
         // one single-CTA launch per replica per step; d_inst_list + g names one
         // instance (instances are independent within a step, so order is free)
-        rc = launch_sweep_kernel(h, 1, s, h->d_inst_list + g, 1, false);
+        rc = launch_sweep_kernel(h, 1, s, h->d_inst_list + g, 1, false,
+                                 step0 + (uint32_t)(done + s), nullptr);
         if (rc) return rc;
       }
     }
@@ -1365,6 +1566,102 @@ int remc_reset_counters(remc_handle* h) {
                                 h->stream));
   REMC_CUDA_TRY(cudaMemsetAsync(h->d_evals_crowd, 0, sizeof(unsigned long long) * h->n_inst,
                                 h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_n_samples, 0, sizeof(int) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_n_bound, 0, sizeof(int) * h->n_inst, h->stream));
+  return REMC_OK;
+}
+
+int remc_set_sampling(remc_handle* h, int sample_every, uint32_t sample_after,
+                      double bound_threshold, int max_records, int max_poses) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (sample_every < 0 || max_records < 0 || max_poses < 0)
+    return set_error(REMC_ERR_INVALID, "negative sampling argument");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if ((unsigned)max_records != h->sample_cap || (unsigned)max_poses != h->pose_cap) {
+    if (h->d_sample_out) cudaFree(h->d_sample_out);
+    if (h->d_pose_out) cudaFree(h->d_pose_out);
+    h->d_sample_out = nullptr;
+    h->d_pose_out = nullptr;
+    h->sample_cap = h->pose_cap = 0;
+    if (max_records > 0 && max_poses > 0) {
+      int rc = dev_alloc(&h->d_sample_out, (size_t)max_records);
+      if (!rc) rc = dev_alloc(&h->d_pose_out, (size_t)max_poses);
+      if (rc) return rc;
+      h->sample_cap = (unsigned)max_records;
+      h->pose_cap = (unsigned)max_poses;
+    }
+  }
+  h->sample_every = sample_every;
+  h->sample_after = sample_after;
+  h->bound_thr = bound_threshold;
+  h->sample_gen++;
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_sample_cursor, 0, sizeof(unsigned) * 4, h->stream));
+  return REMC_OK;
+}
+
+int remc_get_sample_counters(remc_handle* h, int* samples, int* bound) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (samples)
+    REMC_CUDA_TRY(cudaMemcpyAsync(samples, h->d_n_samples, sizeof(int) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (bound)
+    REMC_CUDA_TRY(cudaMemcpyAsync(bound, h->d_n_bound, sizeof(int) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_read_samples(remc_handle* h, remc_sample* records, int max_records,
+                      remc_sample_pose* poses, int max_poses, int* n_records, int* n_poses,
+                      int* n_dropped) {
+  if (!h || !n_records || !n_poses) return set_error(REMC_ERR_INVALID, "null argument");
+  unsigned cur[4] = {0, 0, 0, 0};
+  REMC_CUDA_TRY(cudaMemcpyAsync(cur, h->d_sample_cursor, sizeof(cur), cudaMemcpyDeviceToHost,
+                                h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const unsigned nr = std::min(cur[0], h->sample_cap);
+  // poses of the records kept (a reservation that did not fit wrote nothing)
+  std::vector<SampleHeader> hd(nr);
+  if (nr)
+    REMC_CUDA_TRY(cudaMemcpyAsync(hd.data(), h->d_sample_out, sizeof(SampleHeader) * nr,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  unsigned np = 0;
+  for (unsigned i = 0; i < nr; ++i) np = std::max(np, hd[i].pose_offset + (unsigned)hd[i].n_mol);
+  if ((int)nr > max_records || (int)np > max_poses)
+    return set_error(REMC_ERR_INVALID, "output buffers too small: need %u records, %u poses",
+                     nr, np);
+  for (unsigned i = 0; i < nr; ++i) {
+    records[i].inst = hd[i].inst;
+    records[i].label = hd[i].label;
+    records[i].e_noncrowder = hd[i].e_nc;
+    records[i].e_total = hd[i].e;
+    records[i].temperature = hd[i].temperature;
+    records[i].n_mol = hd[i].n_mol;
+    records[i].pose_offset = (int)hd[i].pose_offset;
+  }
+  if (np) {
+    std::vector<SamplePose> ps(np);
+    REMC_CUDA_TRY(cudaMemcpyAsync(ps.data(), h->d_pose_out, sizeof(SamplePose) * np,
+                                  cudaMemcpyDeviceToHost, h->stream));
+    REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (unsigned i = 0; i < np; ++i) {
+      for (int k = 0; k < 4; ++k) poses[i].q[k] = ps[i].q[k];
+      for (int k = 0; k < 3; ++k) poses[i].centre[k] = ps[i].c[k];
+    }
+  }
+  *n_records = (int)nr;
+  *n_poses = (int)np;
+  if (n_dropped) *n_dropped = (int)cur[2] + (int)(cur[0] - nr);
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_sample_cursor, 0, sizeof(unsigned) * 4, h->stream));
+  return REMC_OK;
+}
+
+int remc_get_noncrowder_energies(remc_handle* h, double* out) {
+  if (!h || !out) return set_error(REMC_ERR_INVALID, "null argument");
+  REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_ecc, sizeof(double) * h->n_inst,
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return REMC_OK;
 }
 
@@ -1435,7 +1732,7 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
   rc = ensure_recs(h, (size_t)steps_per_block);
   if (rc) return rc;
   if (!h->graph_exec || h->graph_steps != steps_per_block || h->graph_seed != seed ||
-      h->graph_recs_gen != h->recs_gen) {
+      h->graph_recs_gen != h->recs_gen || h->graph_sample_gen != h->sample_gen) {
     if (h->graph_exec) {
       cudaGraphExecDestroy(h->graph_exec);
       h->graph_exec = nullptr;
@@ -1458,6 +1755,7 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
     h->graph_steps = steps_per_block;
     h->graph_seed = seed;
     h->graph_recs_gen = h->recs_gen;
+    h->graph_sample_gen = h->sample_gen;
   }
   for (int b = 0; b < n_blocks; ++b) REMC_CUDA_TRY(cudaGraphLaunch(h->graph_exec, h->stream));
   return REMC_OK;

@@ -13,7 +13,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _capi
-from ._capi import MAX_TYPES, NUM_AMINO, Params, SystemDesc, check, lib
+from ._capi import (MAX_TYPES, NUM_AMINO, Params, SamplePose, SampleRecord, SystemDesc, check,
+                    lib)
 from .model import System
 
 
@@ -230,6 +231,42 @@ class Engine:
 
     def reset_counters(self) -> None:
         check(lib().remc_reset_counters(self._h))
+
+    # ------------------------------------------------------------ sampling
+    def set_sampling(self, sample_every: int, sample_after: int = 0,
+                     bound_threshold: float = -1.1844, max_records: int = 0,
+                     max_poses: int = 0) -> None:
+        """Replica::sample inside the sweeps; see remc_set_sampling."""
+        self._max_records, self._max_poses = max_records, max_poses
+        check(lib().remc_set_sampling(self._h, sample_every, sample_after, bound_threshold,
+                                      max_records, max_poses))
+
+    def sample_counters(self):
+        n = np.zeros(self.n_inst, np.int32)
+        b = np.zeros(self.n_inst, np.int32)
+        check(lib().remc_get_sample_counters(self._h, _ptr(n, C.c_int), _ptr(b, C.c_int)))
+        return n, b
+
+    def read_samples(self):
+        """(records, poses, dropped): records as dicts, poses as (n, 7) array
+        of quaternion w,x,y,z and centre x,y,z."""
+        mr = max(1, getattr(self, "_max_records", 0))
+        mp = max(1, getattr(self, "_max_poses", 0))
+        recs = (SampleRecord * mr)()
+        poses = (SamplePose * mp)()
+        nr, npz, nd = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib().remc_read_samples(self._h, recs, mr, poses, mp, C.byref(nr), C.byref(npz),
+                                      C.byref(nd)))
+        out = [{"inst": r.inst, "label": r.label, "e_noncrowder": r.e_noncrowder,
+                "e_total": r.e_total, "temperature": r.temperature, "n_mol": r.n_mol,
+                "pose_offset": r.pose_offset} for r in recs[:nr.value]]
+        arr = np.array([list(p.q) + list(p.centre) for p in poses[:npz.value]], np.float64)
+        return out, arr.reshape(-1, 7), nd.value
+
+    def noncrowder_energies(self) -> np.ndarray:
+        out = np.zeros(self.n_inst, np.float64)
+        check(lib().remc_get_noncrowder_energies(self._h, _ptr(out, C.c_double)))
+        return out
 
     def pair_evaluations(self):
         """(residue-residue, crowder) pair evaluations since the last reset."""
