@@ -181,6 +181,9 @@ def main():
     eng.set_replica_params(w.ladders, np.full(len(w.systems), w.translate_step, np.float32),
                            np.full(len(w.systems), w.rotate_step))
     eng.energy_full()
+    # the project's autotuner picks threads per replica and the shared-memory
+    # layout for this batch (probe sweeps, state restored afterwards)
+    sched_threads, sched_smem, sched_ms = eng.autotune(probe_steps=min(args.block_steps, 256))
     stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=torch.device("cuda", local))
     n_inst = eng.n_inst
     B = args.block_steps
@@ -336,6 +339,9 @@ def main():
                                                      zip(w.systems, w.n_replicas)) / n_inst,
                        "mc_steps_per_bench_step": B, "exchange_every": B,
                        "l2": "256 MB buffer written between timed steps, outside the timing",
+                       "schedule": {"threads_per_replica": sched_threads,
+                                    "molecule_data_in_shared_memory": sched_smem,
+                                    "chosen_by": "remc_autotune"},
                        "parallelism": "replicas" if world == 1 else "weak: %d independent batches" % world},
             "pair_energies_per_s": pair_evals_all / t_max,
             "pair_energy_note": "pair evaluations per second; a dE pair counts twice",

@@ -186,6 +186,17 @@ int remc_delta_energy(remc_handle* h, int inst, int mol, const float* new_pos, d
 int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, uint32_t step0,
              uint32_t round0);
 
+/* Autotuner: times a probe sweep of probe_steps steps for each candidate
+ * schedule (threads per replica 128 or 256; molecule centres and starts in
+ * shared or global memory) on the handle's own systems, restores the state
+ * after every probe, and keeps the fastest. Outputs (may be NULL): the chosen
+ * threads, layout and probe time in ms. No reference counterpart (the
+ * reference fixes its block size by system size, main.cpp:1746-1747). */
+int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads,
+                  int* mol_in_smem, float* best_ms);
+/* Set the sweep schedule directly (threads a multiple of 32, <= 256). */
+int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem);
+
 int remc_sync(remc_handle* h);
 int remc_num_instances(const remc_handle* h);
 const char* remc_last_error_string(void);

@@ -87,6 +87,8 @@ _SIGS = {
                                     C.c_int, PI, PI, PI]),
     "remc_get_noncrowder_energies": (C.c_int, [P, PD]),
     "remc_num_instances": (C.c_int, [P]),
+    "remc_autotune": (C.c_int, [P, C.c_int, C.c_uint64, PI, PI, PF]),
+    "remc_set_schedule": (C.c_int, [P, C.c_int, C.c_int]),
     "remc_last_error_string": (C.c_char_p, []),
 }
 

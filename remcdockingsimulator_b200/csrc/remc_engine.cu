@@ -251,7 +251,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the trial buffer rather than from another thread's not-yet-ordered write.
 // A step of a one-bead molecule therefore costs one barrier; a chain step
 // costs two (trial positions are built by the owners of the chain's beads).
-__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
+__global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
   unsigned long long ev_kh = 0, ev_crowd = 0;
   const int ncb = S.n_chain_beads;  // beads [0, ncb) belong to chains
   const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
+  int to_sample = A.sample_every;  // steps left in the current sampling chunk
   __shared__ long long s_pose_slot;
   __syncthreads();
 
@@ -335,7 +336,17 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
       for (int c = tid; c < chunks; c += nthr) cp_async16(dst + 16 * c, src + 16 * c);
       cp_async_commit();
     }
-    const StepRec rec = s_ring[s & (kRing - 1)];
+    const StepRec& recs_ = s_ring[s & (kRing - 1)];  // stable for the whole step
+    struct {
+      int m, rotate, crowd;
+      float t[3];
+    } rec;
+    rec.m = recs_.m;
+    rec.rotate = recs_.rotate;
+    rec.crowd = recs_.crowd;
+    rec.t[0] = recs_.t[0];
+    rec.t[1] = recs_.t[1];
+    rec.t[2] = recs_.t[2];
     const int m = rec.m;
     const int m0 = mst[m], n = mst[m + 1] - m0;
     const int b = s & 1;
@@ -367,7 +378,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     } else {
       // trial positions of the chain, built by the owners of its beads
       QuatProducts qp{};
-      if (rec.rotate) qp = quat_products(rec.q[0], rec.q[1], rec.q[2], rec.q[3]);
+      if (rec.rotate) qp = quat_products(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3]);
       int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
       for (; j < m0 + n; j += nthr) {
         const int k = j - m0;
@@ -389,6 +400,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     // for a chain, the part from other chains' beads (j < ncb) is kept apart:
     // it is the change of the chain-chain energy sample() adds
     double dacc = 0.0, dcc = 0.0;
+    const bool split = !rec.crowd && ncb < N;
     if (!skip) {
       for (int k = 0; k < n; ++k) {
         float4 pold, pnew;
@@ -403,36 +415,44 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
         const bool a_crowd = ta >= kNumAmino;
         const float4* trow = s_tab + ta * kNT;
         float acc_c = 0.0f, acc_o = 0.0f;
-        int j = tid;
-        for (; j < ncb; j += nthr) {
-          if (j >= m0 && j < m0 + n) continue;
-          const float4 pj = s_beads[j];
-          const int tb = bead_type(pj.w);
-          const float4 Tj = trow[tb];
-          const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, a_crowd, A.K);
-          const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, a_crowd, A.K);
-          acc_c += en - eo;
-        }
-        for (; j < N; j += nthr) {
-          if (j >= m0 && j < m0 + n) continue;
-          const float4 pj = s_beads[j];
-          const int tb = bead_type(pj.w);
-          const float4 Tj = trow[tb];
-          const bool crowd = a_crowd || tb >= kNumAmino;
-          const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
-          const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
-          acc_o += en - eo;
-        }
-        if (a_crowd) {
-          dacc += (double)acc_c + (double)acc_o;
-        } else {
+        if (split) {
+          // a chain in a crowded system: other chains' beads first (j < ncb)
+          int j = tid;
+          for (; j < ncb; j += nthr) {
+            if (j >= m0 && j < m0 + n) continue;
+            const float4 pj = s_beads[j];
+            const float4 Tj = trow[bead_type(pj.w)];
+            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, false, A.K);
+            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, false, A.K);
+            acc_c += en - eo;
+          }
+          for (; j < N; j += nthr) {
+            const float4 pj = s_beads[j];
+            const float4 Tj = trow[bead_type(pj.w)];
+            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, true, A.K);
+            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, true, A.K);
+            acc_o += en - eo;
+          }
           dcc += (double)acc_c;
-          dacc += (double)acc_o;
+        } else {
+          for (int j = tid; j < N; j += nthr) {
+            if (j >= m0 && j < m0 + n) continue;
+            const float4 pj = s_beads[j];
+            const int tb = bead_type(pj.w);
+            const float4 Tj = trow[tb];
+            const bool crowd = a_crowd || tb >= kNumAmino;
+            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
+            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
+            acc_o += en - eo;
+          }
         }
+        dacc += (double)acc_o;
       }
+      // without crowders every pair of a chain move is a chain-chain pair
+      if (!rec.crowd && !split) dcc = dacc;
     }
     dacc = warp_sum(dacc);
-    if (!rec.crowd) dcc = warp_sum(dcc);
+    if (split) dcc = warp_sum(dcc);
     if (lane == 0) {
       s_red[b * 64 + warp] = dacc;
       s_red[b * 64 + 32 + warp] = dcc;
@@ -442,11 +462,14 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
 
     // ---- every thread: the same FP64 sums and the same Metropolis decision
     double dE_cc = 0.0, dE = 0.0;
-    if (!rec.crowd)
-      for (int w = 0; w < nwarps; ++w) dE_cc += s_red[b * 64 + 32 + w];
     for (int w = 0; w < nwarps; ++w) dE += s_red[b * 64 + w];
-    dE += dE_cc;
-    const int acc = dE < 0.0 ? 1 : (dE < rec.thr ? 2 : 0);
+    if (split) {
+      for (int w = 0; w < nwarps; ++w) dE_cc += s_red[b * 64 + 32 + w];
+      dE += dE_cc;
+    } else if (!rec.crowd) {
+      dE_cc = dE;  // no crowders: the whole change is chain-chain
+    }
+    const int acc = dE < 0.0 ? 1 : (dE < recs_.thr ? 2 : 0);
     if (acc) {
       energy += dE;
       ecc += dE_cc;
@@ -456,7 +479,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
       } else {
         // the owners install the chain (and its relative positions)
         QuatProducts qp{};
-        if (rec.rotate) qp = quat_products(rec.q[0], rec.q[1], rec.q[2], rec.q[3]);
+        if (rec.rotate) qp = quat_products(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3]);
         int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
         for (; j < m0 + n; j += nthr) {
           s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
@@ -472,7 +495,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
         if (rec.rotate) {
           double* qd = A.quat + 4 * (size_t)(mol_off + m);
           double out[4];
-          quat_mul(rec.q[0], rec.q[1], rec.q[2], rec.q[3], qd[0], qd[1], qd[2], qd[3], out);
+          quat_mul(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3], qd[0], qd[1], qd[2], qd[3], out);
           qd[0] = out[0];
           qd[1] = out[1];
           qd[2] = out[2];
@@ -496,7 +519,8 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs A) {
     }
     // ---- Replica::sample at the end of every sampling chunk (main.cpp:975-989):
     // bound if potential (+ chain-chain energy when crowders exist) < threshold
-    if (A.sample_every > 0 && ((s + 1) % A.sample_every) == 0) {
+    if (to_sample > 0 && --to_sample == 0) {
+      to_sample = A.sample_every;
       const uint32_t label = step0 + (uint32_t)(s + 1 - A.sample_every);
       if (label >= A.sample_after) {
         const double enc = (ncb < N) ? energy + ecc : energy;
@@ -713,6 +737,15 @@ __global__ void exchange_kernel(const SysDev* __restrict__ sys, const float* __r
   }
 }
 
+// Set the device step/round/offset counters from kernel arguments (stream
+// ordered, no host copy).
+__global__ void ctrl_set_kernel(uint32_t* ctrl, uint32_t step0, uint32_t round0) {
+  ctrl[0] = step0;
+  ctrl[1] = round0;
+  ctrl[2] = round0 & 1u;
+  ctrl[3] = 0u;
+}
+
 // Advance the device step/round/offset counters between graph replays.
 __global__ void ctrl_advance_kernel(uint32_t* ctrl, uint32_t steps) {
   ctrl[0] += steps;
@@ -811,6 +844,8 @@ struct remc_handle {
   int* d_queue = nullptr;
   int sweep_grid = 0;  // resident CTAs of the persistent sweep
   int mol_in_smem = 1; // molecule centres/starts in shared memory (else global)
+  int max_dyn_smem = 0;
+  int config_gen = 0;  // bumped when the sweep schedule changes
   TileItem* d_items = nullptr;
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
@@ -837,6 +872,7 @@ struct remc_handle {
   uint64_t graph_seed = 0;
   int graph_recs_gen = -1;
   int graph_sample_gen = -1;
+  int graph_config_gen = -1;
 };
 
 namespace {
@@ -936,6 +972,28 @@ int ensure_recs(remc_handle* h, size_t steps) {
   if (rc) return rc;
   h->recs_cap = steps;
   h->recs_gen++;
+  return REMC_OK;
+}
+
+// Set the sweep schedule: threads per replica and where molecule data lives.
+int configure_sweep(remc_handle* h, int threads, int mol_in_smem) {
+  if (threads % 32 != 0 || threads < 32 || threads > 256)
+    return set_error(REMC_ERR_INVALID, "threads per replica must be a multiple of 32, <= 256");
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem).total;
+  if (smem > (size_t)h->max_dyn_smem)
+    return set_error(REMC_ERR_INVALID,
+                     "largest system needs %zu bytes of shared memory, device allows %d", smem,
+                     h->max_dyn_smem);
+  int per_sm = 0;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel, threads, smem);
+  if (e != cudaSuccess || per_sm < 1)
+    return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
+                     cudaGetErrorString(e));
+  h->sweep_threads = threads;
+  h->mol_in_smem = mol_in_smem;
+  h->sweep_grid = per_sm * h->num_sms;
+  h->config_gen++;
   return REMC_OK;
 }
 
@@ -1165,34 +1223,22 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     return set_error(REMC_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
   }
   const int max_dyn = max_smem - (int)fattr.sharedSizeBytes;
-  size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, 1).total;
-  if (smem > (size_t)max_dyn) {
-    h->mol_in_smem = 0;
-    smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, 0).total;
-  }
-  if (smem > (size_t)max_dyn) {
-    delete h;
-    return set_error(REMC_ERR_INVALID,
-                     "largest system needs %zu bytes of shared memory, device allows %d", smem,
-                     max_dyn);
-  }
+  h->max_dyn_smem = max_dyn;
   e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn);
   if (e != cudaSuccess) {
     delete h;
     return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
   }
-  // larger systems get more threads per replica
-  h->sweep_threads = h->nmax <= 2048 ? 128 : 256;
+  // default schedule (the autotuner may replace it): molecule data in shared
+  // memory when it fits, more threads per replica for larger systems
   {
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel, h->sweep_threads,
-                                                      smem);
-    if (e != cudaSuccess || per_sm < 1) {
+    const int threads = h->nmax <= 2048 ? 128 : 256;
+    int rc0 = configure_sweep(h, threads, 1);
+    if (rc0) rc0 = configure_sweep(h, threads, 0);
+    if (rc0) {
       delete h;
-      return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
-                       cudaGetErrorString(e));
+      return rc0;
     }
-    h->sweep_grid = per_sm * h->num_sms;
   }
   // ---- work list of the full-energy kernel (upper-triangle tiles)
   std::vector<TileItem> items;
@@ -1725,14 +1771,15 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
   if (n_blocks < 0 || steps_per_block <= 0)
     return set_error(REMC_ERR_INVALID, "bad block counts");
   // device control block: step counter, round counter, offset parity
-  uint32_t ctrl[4] = {step0, round0, round0 & 1u, 0u};
-  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
+  ctrl_set_kernel<<<1, 1, 0, h->stream>>>(h->d_ctrl, step0, round0);
+  REMC_CUDA_TRY(cudaGetLastError());
   if ((size_t)steps_per_block > max_chunk_steps(h))
     return set_error(REMC_ERR_INVALID, "steps_per_block too large for the record buffer");
   rc = ensure_recs(h, (size_t)steps_per_block);
   if (rc) return rc;
   if (!h->graph_exec || h->graph_steps != steps_per_block || h->graph_seed != seed ||
-      h->graph_recs_gen != h->recs_gen || h->graph_sample_gen != h->sample_gen) {
+      h->graph_recs_gen != h->recs_gen || h->graph_sample_gen != h->sample_gen ||
+      h->graph_config_gen != h->config_gen) {
     if (h->graph_exec) {
       cudaGraphExecDestroy(h->graph_exec);
       h->graph_exec = nullptr;
@@ -1756,9 +1803,99 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
     h->graph_seed = seed;
     h->graph_recs_gen = h->recs_gen;
     h->graph_sample_gen = h->sample_gen;
+    h->graph_config_gen = h->config_gen;
   }
   for (int b = 0; b < n_blocks; ++b) REMC_CUDA_TRY(cudaGraphLaunch(h->graph_exec, h->stream));
   return REMC_OK;
+}
+
+int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_out,
+                  int* mol_in_smem_out, float* best_ms_out) {
+  int rc = check_ready(h);
+  if (rc) return rc;
+  if (probe_steps <= 0) return set_error(REMC_ERR_INVALID, "probe_steps must be positive");
+  // snapshot everything a sweep changes, so tuning leaves the state as it was
+  struct Buf {
+    void* dev;
+    size_t bytes;
+    void* save;
+  };
+  Buf bufs[] = {{h->d_pos, sizeof(float4) * h->total_beads, nullptr},
+                {h->d_rel, sizeof(float4) * h->total_beads, nullptr},
+                {h->d_centre, sizeof(float4) * h->total_mols, nullptr},
+                {h->d_quat, sizeof(double) * 4 * h->total_mols, nullptr},
+                {h->d_energy, sizeof(double) * h->n_inst, nullptr},
+                {h->d_ecc, sizeof(double) * h->n_inst, nullptr},
+                {h->d_acc_neg, sizeof(int) * h->n_inst, nullptr},
+                {h->d_acc_boltz, sizeof(int) * h->n_inst, nullptr},
+                {h->d_rej, sizeof(int) * h->n_inst, nullptr},
+                {h->d_evals_kh, sizeof(unsigned long long) * h->n_inst, nullptr},
+                {h->d_evals_crowd, sizeof(unsigned long long) * h->n_inst, nullptr},
+                {h->d_n_samples, sizeof(int) * h->n_inst, nullptr},
+                {h->d_n_bound, sizeof(int) * h->n_inst, nullptr}};
+  const int nb = (int)(sizeof(bufs) / sizeof(bufs[0]));
+  auto release = [&]() {
+    for (int i = 0; i < nb; ++i)
+      if (bufs[i].save) cudaFree(bufs[i].save);
+  };
+  for (int i = 0; i < nb; ++i) {
+    if (cudaMalloc(&bufs[i].save, bufs[i].bytes) != cudaSuccess) {
+      release();
+      return set_error(REMC_ERR_NOMEM, "autotune snapshot allocation failed");
+    }
+    REMC_CUDA_TRY(cudaMemcpyAsync(bufs[i].save, bufs[i].dev, bufs[i].bytes,
+                                  cudaMemcpyDeviceToDevice, h->stream));
+  }
+  const int saved_every = h->sample_every;
+  h->sample_every = 0;
+  rc = ensure_recs(h, (size_t)probe_steps);
+  const int cand_threads[2] = {128, 256};
+  int best_t = h->sweep_threads, best_m = h->mol_in_smem;
+  float best = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int ti = 0; ti < 2 && !rc; ++ti) {
+    for (int mi = 1; mi >= 0 && !rc; --mi) {
+      if (configure_sweep(h, cand_threads[ti], mi) != REMC_OK) continue;
+      float ms = 0.0f;
+      for (int rep = 0; rep < 2 && !rc; ++rep) {  // first launch warms up
+        cudaEventRecord(e0, h->stream);
+        rc = launch_sweep(h, probe_steps, seed, 0, nullptr);
+        cudaEventRecord(e1, h->stream);
+        if (!rc && cudaEventSynchronize(e1) != cudaSuccess)
+          rc = set_error(REMC_ERR_CUDA, "autotune probe failed");
+        if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+        for (int i = 0; i < nb && !rc; ++i)
+          if (cudaMemcpyAsync(bufs[i].dev, bufs[i].save, bufs[i].bytes, cudaMemcpyDeviceToDevice,
+                              h->stream) != cudaSuccess)
+            rc = set_error(REMC_ERR_CUDA, "autotune restore failed");
+      }
+      if (!rc && ms < best) {
+        best = ms;
+        best_t = cand_threads[ti];
+        best_m = mi;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->sample_every = saved_every;
+  cudaStreamSynchronize(h->stream);
+  release();
+  if (rc) return rc;
+  rc = configure_sweep(h, best_t, best_m);
+  if (rc) return rc;
+  if (threads_out) *threads_out = best_t;
+  if (mol_in_smem_out) *mol_in_smem_out = best_m;
+  if (best_ms_out) *best_ms_out = best;
+  return REMC_OK;
+}
+
+int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return configure_sweep(h, threads, mol_in_smem ? 1 : 0);
 }
 
 int remc_sync(remc_handle* h) {

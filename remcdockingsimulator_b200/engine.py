@@ -275,6 +275,17 @@ class Engine:
         check(lib().remc_get_pair_evaluations(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def autotune(self, probe_steps: int = 200, seed: int = 12345):
+        """Pick the fastest sweep schedule for these systems (remc_autotune);
+        returns (threads, molecule data in shared memory, probe ms)."""
+        t, m, ms = C.c_int(0), C.c_int(0), C.c_float(0.0)
+        check(lib().remc_autotune(self._h, probe_steps, seed, C.byref(t), C.byref(m),
+                                  C.byref(ms)))
+        return t.value, bool(m.value), ms.value
+
+    def set_schedule(self, threads: int, mol_in_smem: bool) -> None:
+        check(lib().remc_set_schedule(self._h, threads, 1 if mol_in_smem else 0))
+
     def stream_ptr(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         s = C.c_void_p(0)

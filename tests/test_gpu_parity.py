@@ -273,3 +273,36 @@ def test_bad_inputs_are_rejected(built_lib):
             eng.sweep(10, 1, 0)  # replica parameters not set yet
         with pytest.raises(RemcError):
             eng.set_replica_params([np.array([300.0, 290.0], np.float32)], [0.5, 0.5], [0.2, 0.2])
+
+
+def test_autotune_restores_state_and_schedules_agree(built_lib):
+    """The autotuner leaves the state untouched, and every schedule gives the
+    same trajectory."""
+    from remcdockingsimulator_b200 import synth
+    w = synth.crowded(14)
+    s = w.systems[0]
+    R = 4
+    outs = []
+    for sched in ("tuned", (128, True), (256, False)):
+        with _engine([s], R, w.params) as eng:
+            eng.set_replica_params([w.ladders[0][:R]], np.full(R, 0.5, np.float32),
+                                   np.full(R, 0.2))
+            eng.energy_full()
+            before = eng.download_state()
+            e_before = eng.energies()
+            if sched == "tuned":
+                t, m, ms = eng.autotune(probe_steps=64)
+                assert t in (128, 256) and ms > 0
+                after = eng.download_state()
+                for a, b in zip(before, after):
+                    assert np.array_equal(a, b)
+                assert np.array_equal(e_before, eng.energies())
+                assert all(c.sum() == 0 for c in eng.counters())
+            else:
+                eng.set_schedule(*sched)
+            eng.sweep(400, 11, 0)
+            outs.append((eng.download_state(), eng.energies()))
+    for o in outs[1:]:
+        for a, b in zip(outs[0][0], o[0]):
+            assert np.array_equal(a, b)
+        assert np.allclose(outs[0][1], o[1], rtol=1e-9, atol=1e-9)

@@ -80,6 +80,7 @@ def test_driver_writes_reference_output_files(tmp_path, built_lib):
                         os.path.join(d, "output")])
     a.pid = 4242
     mols = remc.load_config(a, table, log=lambda *_: None)
+    remc.parse_cli(["-f", cfg, "-r", "6"], a)  # flags override the file, as main() does
     a.sample_after = 0
     remc.write_file_index(a)
     from remcdockingsimulator_b200.model import System
