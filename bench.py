@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-snapshots", type=int, default=4096,
+                    help="snapshots of the crowded system for the adjoint/energy cost ratio")
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MC steps of the per-replica-launch comparison sample")
     return ap.parse_args()
@@ -320,6 +322,39 @@ def main():
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
            "path": "remc_upload_state + remc_run + remc_download_state + remc_get_energies"}
 
+    # ---- adjoint cost against one energy evaluation: 4096 snapshots of the
+    # crowded system (all replicas of one system, decorrelated by a sweep)
+    adjoint = None
+    if args.adjoint_snapshots > 0:
+        wa = synth.crowded(args.seed + 7 + 1000 * rank)
+        ea = Engine(wa.systems, [args.adjoint_snapshots], wa.params)
+        ea.set_replica_params([np.linspace(290, 480, args.adjoint_snapshots).astype(np.float32)],
+                              [wa.translate_step], [wa.rotate_step])
+        ea.energy_full()
+        ea.sweep(200, seed + 9, 0)
+        ea.sync()
+        sa = torch.cuda.ExternalStream(ea.stream_ptr(), device=torch.device("cuda", local))
+        times = {}
+        for name, fn in (("energy", lambda: ea.energy_full_async()),
+                         ("adjoint", lambda: ea.adjoint_kernels())):
+            fn()
+            ea.sync()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(sa):
+                a0.record(sa)
+            for _ in range(5):
+                fn()
+            with torch.cuda.stream(sa):
+                a1.record(sa)
+            ea.sync()
+            times[name] = a0.elapsed_time(a1) / 5
+        adjoint = {"snapshots": args.adjoint_snapshots, "energy_ms": times["energy"],
+                   "adjoint_ms": times["adjoint"],
+                   "adjoint_over_energy": times["adjoint"] / times["energy"],
+                   "outputs": "per-bead forces, per-molecule force+torque, dE/dlambda, "
+                              "dE/dXi, dE/deps[20x20]"}
+        ea.close()
+
     # ---- CPU baseline (reference engine, bounded sample), rank 0 at N = 1
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -346,6 +381,7 @@ def main():
             "pair_energies_per_s": pair_evals_all / t_max,
             "pair_energy_note": "pair evaluations per second; a dE pair counts twice",
             "roofline": roofline, "plain": plain, "e2e": e2e, "cpu_baseline": cpu,
+            "adjoint": adjoint,
             "clocks": clk, "gpu_launches": gpu_launches,
         }
         print(json.dumps(line))

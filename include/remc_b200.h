@@ -172,6 +172,20 @@ int remc_read_samples(remc_handle* h, remc_sample* records, int max_records,
  * over chain pairs, Replica.cpp:793-828), tracked with the running energy. */
 int remc_get_noncrowder_energies(remc_handle* h, double* out);
 
+/* Adjoint of the full energy of every instance (no reference counterpart:
+ * the reference has no gradients). Outputs (host, any may be NULL):
+ *   forces[3 per bead per instance]      F = -dE/dr (FP32, kcal/mol/A)
+ *   mol_force_torque[6 per molecule]     sum F and torque sum rel x F about
+ *                                        the centre (FP64)
+ *   dE_dlambda[n_inst], dE_dxi[n_inst]   kcal/mol per unit lambda / per A
+ *   dE_deps[400 per instance]            derivative with respect to the
+ *                                        symmetric contact energy eps_ab
+ *                                        (entries ab and ba both hold it)
+ *   energy[n_inst]                       the energy the adjoint saw
+ * Forces are summed with FP32 atomics (order-dependent in the last bits). */
+int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
+                        double* dE_dlambda, double* dE_dxi, double* dE_deps, double* energy);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after the engine's. */
 int remc_get_stream(remc_handle* h, void** stream);

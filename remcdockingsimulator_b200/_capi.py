@@ -86,6 +86,7 @@ _SIGS = {
     "remc_read_samples": (C.c_int, [P, C.POINTER(SampleRecord), C.c_int, C.POINTER(SamplePose),
                                     C.c_int, PI, PI, PI]),
     "remc_get_noncrowder_energies": (C.c_int, [P, PD]),
+    "remc_energy_adjoint": (C.c_int, [P, PF, PD, PD, PD, PD, PD]),
     "remc_num_instances": (C.c_int, [P]),
     "remc_autotune": (C.c_int, [P, C.c_int, C.c_uint64, PI, PI, PF]),
     "remc_set_schedule": (C.c_int, [P, C.c_int, C.c_int]),

@@ -695,6 +695,185 @@ __global__ void energy_reduce_kernel(const int* __restrict__ item_off, int n_ins
   }
 }
 
+
+// ------------------------------------------------------------------ adjoint
+// Forces and parameter derivatives of the full energy: same upper-triangle
+// items as energy_tile_kernel. Thread i keeps its bead's force in registers;
+// the force on each j bead is warp-reduced per j into per-warp shared rows and
+// added to global memory once per item. dE/deps comes from the per-type-pair
+// sums G_ab = sum d e / d eps_ab (eps enters each residue pair linearly),
+// dE/dXi from sum e_DH r / Xi^2.
+struct AdjConsts {
+  float inv_xi;   // 1/Xi
+  float c_lj;     // LJ_CF * KBT_CF (d e / d eps per unit of the 4 s6 (1 - s6) form)
+  float inv_xi2;  // 1/Xi^2
+};
+
+__global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
+    const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
+    const float4* __restrict__ pos, const float4* __restrict__ tab,
+    const TileItem* __restrict__ items, int n_items, float* __restrict__ forces,
+    double* __restrict__ G, double* __restrict__ dxi, double* __restrict__ e_out,
+    EnergyConsts K, AdjConsts C) {
+  __shared__ float4 s_tab[kNT * kNT];
+  __shared__ float4 s_j[kTile];
+  __shared__ float s_fj[kTile / 32][kTile][3];
+  __shared__ float s_G[kNumAmino * kNumAmino];
+  __shared__ double s_red[kTile / 32][2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const TileItem W = items[it];
+    const SysDev S = sys[inst_sys[W.inst]];
+    const int N = S.n_beads;
+    const int base = S.bead_base + (W.inst - S.inst0) * N;
+    const float box = S.box, invbox = S.invbox;
+    const int j0 = W.tj * kTile;
+    const int jn = min(kTile, N - j0);
+    __syncthreads();  // the previous item is done with the shared buffers
+    if (tid < jn) s_j[tid] = pos[base + j0 + tid];
+    for (int k = tid; k < (kTile / 32) * kTile * 3; k += kTile) (&s_fj[0][0][0])[k] = 0.0f;
+    for (int k = tid; k < kNumAmino * kNumAmino; k += kTile) s_G[k] = 0.0f;
+    __syncthreads();
+    const int i = W.ti * kTile + tid;
+    const bool ivalid = i < N;
+    float4 pi = ivalid ? pos[base + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ta = bead_type(pi.w), mi = ivalid ? bead_mol(pi.w) : -1;
+    const bool a_crowd = ta >= kNumAmino;
+    float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
+    for (int jj = 0; jj < jn; ++jj) {  // uniform trip count: the j force is warp-reduced
+      const float4 pj = s_j[jj];
+      const int tb = bead_type(pj.w);
+      const bool valid = ivalid && (W.ti != W.tj || jj > tid) && bead_mol(pj.w) != mi;
+      float gx = 0.f, gy = 0.f, gz = 0.f;
+      if (valid) {
+        const float dx = min_image(pi.x - pj.x, box, invbox);
+        const float dy = min_image(pi.y - pj.y, box, invbox);
+        const float dz = min_image(pi.z - pj.z, box, invbox);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float rinv = fast_rsqrt(r2);
+        const float rinv2 = rinv * rinv;
+        const float4 T = s_tab[tb * kNT + ta];
+        float f;  // -(de/dr)/r
+        if (a_crowd || tb >= kNumAmino) {
+          const float i6 = rinv2 * rinv2 * rinv2;
+          float e = T.x * i6;
+          float p = 6.0f;
+          if (K.crowder_mode) {
+            e *= i6;
+            p = 12.0f;
+          }
+          if (!(r2 < T.z)) e = 0.0f;
+          acc_e += e;
+          f = p * e * rinv2;
+        } else {
+          const float s2 = T.y * rinv2;
+          const float s6 = s2 * s2 * s2;
+          const float g = fmaf(-s6, s6, s6);           // s6 (1 - s6)
+          float lj = T.x * g;
+          float dlj = 6.0f * T.x * s6 * fmaf(-2.0f, s6, 1.0f) * rinv2;  // -(dLJ/dr)/r
+          float dg = 4.0f * g;                          // d e_LJ / d eps per c_lj
+          if (r2 < T.z) {
+            lj = fmaf(0.5f, T.x, -lj);
+            dlj = -dlj;
+            dg = 2.0f - dg;
+          }
+          const float r = r2 * rinv;
+          const float dh = T.w * fast_ex2(r * K.c_xi) * rinv;
+          acc_e += lj + dh;
+          acc_x += dh * r;                               // * 1/Xi^2 below
+          f = dlj + dh * (C.inv_xi + rinv) * rinv;
+          if (ta < kNumAmino && tb < kNumAmino) atomicAdd(&s_G[ta * kNumAmino + tb], dg * C.c_lj);
+        }
+        gx = f * dx;
+        gy = f * dy;
+        gz = f * dz;
+        fx += gx;
+        fy += gy;
+        fz += gz;
+      }
+      // force on j = -(sum over this warp's i of the force on i from j)
+      for (int off = 16; off > 0; off >>= 1) {
+        gx += __shfl_down_sync(0xffffffffu, gx, off);
+        gy += __shfl_down_sync(0xffffffffu, gy, off);
+        gz += __shfl_down_sync(0xffffffffu, gz, off);
+      }
+      if (lane == 0) {
+        s_fj[warp][jj][0] -= gx;
+        s_fj[warp][jj][1] -= gy;
+        s_fj[warp][jj][2] -= gz;
+      }
+    }
+    double de = warp_sum((double)acc_e), dxv = warp_sum((double)acc_x);
+    if (lane == 0) {
+      s_red[warp][0] = de;
+      s_red[warp][1] = dxv;
+    }
+    __syncthreads();
+    if (ivalid) {
+      atomicAdd(&forces[3 * (size_t)(base + i)], fx);
+      atomicAdd(&forces[3 * (size_t)(base + i) + 1], fy);
+      atomicAdd(&forces[3 * (size_t)(base + i) + 2], fz);
+    }
+    if (tid < jn) {
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      for (int w = 0; w < kTile / 32; ++w) {
+        sx += s_fj[w][tid][0];
+        sy += s_fj[w][tid][1];
+        sz += s_fj[w][tid][2];
+      }
+      atomicAdd(&forces[3 * (size_t)(base + j0 + tid)], sx);
+      atomicAdd(&forces[3 * (size_t)(base + j0 + tid) + 1], sy);
+      atomicAdd(&forces[3 * (size_t)(base + j0 + tid) + 2], sz);
+    }
+    for (int k = tid; k < kNumAmino * kNumAmino; k += kTile)
+      if (s_G[k] != 0.0f) atomicAdd(&G[(size_t)W.inst * kNumAmino * kNumAmino + k], (double)s_G[k]);
+    if (tid == 0) {
+      double e = 0.0, x = 0.0;
+      for (int w = 0; w < kTile / 32; ++w) {
+        e += s_red[w][0];
+        x += s_red[w][1];
+      }
+      atomicAdd(&e_out[W.inst], e);
+      atomicAdd(&dxi[W.inst], x * (double)C.inv_xi2);
+    }
+  }
+}
+
+// Per-molecule force and torque about the centre (torque = sum rel x F):
+// one CTA per instance, one warp per molecule, FP64 sums.
+__global__ void molecule_force_torque_kernel(const SysDev* __restrict__ sys,
+                                             const int* __restrict__ inst_sys,
+                                             const int* __restrict__ mol_start,
+                                             const float4* __restrict__ rel,
+                                             const float* __restrict__ forces,
+                                             double* __restrict__ out) {
+  const int inst = blockIdx.x;
+  const SysDev S = sys[inst_sys[inst]];
+  const int slot = inst - S.inst0;
+  const int base = S.bead_base + slot * S.n_beads;
+  const int mbase = S.mol_base + slot * S.n_mol;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int m = warp; m < S.n_mol; m += nw) {
+    const int a = mol_start[S.mstart_off + m], b = mol_start[S.mstart_off + m + 1];
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = a + lane; k < b; k += 32) {
+      const float4 rl = rel[base + k];
+      const double Fx = forces[3 * (size_t)(base + k)], Fy = forces[3 * (size_t)(base + k) + 1],
+                   Fz = forces[3 * (size_t)(base + k) + 2];
+      v[0] += Fx;
+      v[1] += Fy;
+      v[2] += Fz;
+      v[3] += (double)rl.y * Fz - (double)rl.z * Fy;
+      v[4] += (double)rl.z * Fx - (double)rl.x * Fz;
+      v[5] += (double)rl.x * Fy - (double)rl.y * Fx;
+    }
+    for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
+    if (lane == 0)
+      for (int c = 0; c < 6; ++c) out[6 * (size_t)(mbase + m) + c] = v[c];
+  }
+}
+
 // ------------------------------------------------------------------ exchange
 __global__ void exchange_kernel(const SysDev* __restrict__ sys, const float* __restrict__ ladder,
                                 const double* __restrict__ energy, int* __restrict__ temp_idx,
@@ -850,6 +1029,11 @@ struct remc_handle {
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
   double* d_scratch_cc = nullptr;
+  float* d_forces = nullptr;   // adjoint outputs (allocated on first use)
+  double* d_G = nullptr;
+  double* d_dxi = nullptr;
+  double* d_eadj = nullptr;
+  double* d_mft = nullptr;
   double* d_ecc = nullptr;
   int* d_n_samples = nullptr;
   int* d_n_bound = nullptr;
@@ -894,7 +1078,8 @@ void free_all(remc_handle* h) {
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
                   h->d_evals_kh, h->d_evals_crowd, h->d_mol_role, h->d_mrole_off, h->d_recs,
                   h->d_queue,      h->d_scratch_cc, h->d_ecc,     h->d_n_samples,  h->d_n_bound,
-                  h->d_sample_out, h->d_pose_out, h->d_sample_cursor,
+                  h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_forces, h->d_G,
+                  h->d_dxi,        h->d_eadj,     h->d_mft,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE};
   for (void* p : ptrs)
@@ -1700,6 +1885,74 @@ int remc_read_samples(remc_handle* h, remc_sample* records, int max_records,
   *n_poses = (int)np;
   if (n_dropped) *n_dropped = (int)cur[2] + (int)(cur[0] - nr);
   REMC_CUDA_TRY(cudaMemsetAsync(h->d_sample_cursor, 0, sizeof(unsigned) * 4, h->stream));
+  return REMC_OK;
+}
+
+int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
+                        double* dE_dlambda, double* dE_dxi, double* dE_deps, double* energy) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
+  int rc = REMC_OK;
+  if (!h->d_forces) {
+    rc = dev_alloc(&h->d_forces, 3 * h->total_beads);
+    if (!rc) rc = dev_alloc(&h->d_G, (size_t)kNumAmino * kNumAmino * h->n_inst);
+    if (!rc) rc = dev_alloc(&h->d_dxi, h->n_inst);
+    if (!rc) rc = dev_alloc(&h->d_eadj, h->n_inst);
+    if (!rc) rc = dev_alloc(&h->d_mft, 6 * h->total_mols);
+    if (rc) return rc;
+  }
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_forces, 0, sizeof(float) * 3 * h->total_beads, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_G, 0, sizeof(double) * kNumAmino * kNumAmino * h->n_inst,
+                                h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_dxi, 0, sizeof(double) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_eadj, 0, sizeof(double) * h->n_inst, h->stream));
+  AdjConsts C;
+  C.inv_xi = 1.0f / h->params.debye_length;
+  C.inv_xi2 = C.inv_xi * C.inv_xi;
+  C.c_lj = (float)((double)h->params.lj_cf * (double)h->params.kbt_cf);
+  const int grid = std::min(h->n_items, h->num_sms * 8);
+  adjoint_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
+                                                    h->d_items, h->n_items, h->d_forces, h->d_G,
+                                                    h->d_dxi, h->d_eadj, consts_of(h), C);
+  REMC_CUDA_TRY(cudaGetLastError());
+  molecule_force_torque_kernel<<<h->n_inst, 256, 0, h->stream>>>(
+      h->d_sys, h->d_inst_sys, h->d_mol_start, h->d_rel, h->d_forces, h->d_mft);
+  REMC_CUDA_TRY(cudaGetLastError());
+  if (forces)
+    REMC_CUDA_TRY(cudaMemcpyAsync(forces, h->d_forces, sizeof(float) * 3 * h->total_beads,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (mol_force_torque)
+    REMC_CUDA_TRY(cudaMemcpyAsync(mol_force_torque, h->d_mft, sizeof(double) * 6 * h->total_mols,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (dE_dxi)
+    REMC_CUDA_TRY(cudaMemcpyAsync(dE_dxi, h->d_dxi, sizeof(double) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  if (energy)
+    REMC_CUDA_TRY(cudaMemcpyAsync(energy, h->d_eadj, sizeof(double) * h->n_inst,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> G;
+  if (dE_deps || dE_dlambda) {
+    G.resize((size_t)kNumAmino * kNumAmino * h->n_inst);
+    REMC_CUDA_TRY(cudaMemcpyAsync(G.data(), h->d_G, sizeof(double) * G.size(),
+                                  cudaMemcpyDeviceToHost, h->stream));
+  }
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  // symmetric parameter eps_ab = eps_ba: both table entries carry the full
+  // derivative; eps = lambda (M - e0) gives dE/dlambda = sum G_ab (M_ab - e0)
+  for (int g = 0; g < h->n_inst && !G.empty(); ++g) {
+    const double* Gi = &G[(size_t)g * kNumAmino * kNumAmino];
+    double dl = 0.0;
+    for (int a = 0; a < kNumAmino; ++a) {
+      for (int b = 0; b < kNumAmino; ++b) {
+        const double d = (a == b) ? Gi[a * kNumAmino + a]
+                                  : Gi[a * kNumAmino + b] + Gi[b * kNumAmino + a];
+        if (dE_deps) dE_deps[(size_t)g * kNumAmino * kNumAmino + a * kNumAmino + b] = d;
+        dl += Gi[a * kNumAmino + b] *
+              ((double)h->pair_table[a * 20 + b] - (double)h->params.e0);
+      }
+    }
+    if (dE_dlambda) dE_dlambda[g] = dl;
+  }
   return REMC_OK;
 }
 

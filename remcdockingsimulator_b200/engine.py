@@ -263,6 +263,31 @@ class Engine:
         arr = np.array([list(p.q) + list(p.centre) for p in poses[:npz.value]], np.float64)
         return out, arr.reshape(-1, 7), nd.value
 
+    def adjoint(self):
+        """Forces, per-molecule force/torque, dE/dlambda, dE/dXi, dE/deps[20x20]
+        and the energy of every instance (remc_energy_adjoint)."""
+        nb = sum(s.n_beads * r for s, r in zip(self.systems, self.n_replicas))
+        nm = sum(s.n_mol * r for s, r in zip(self.systems, self.n_replicas))
+        f = np.zeros((nb, 3), np.float32)
+        ft = np.zeros((nm, 6), np.float64)
+        dl = np.zeros(self.n_inst)
+        dx = np.zeros(self.n_inst)
+        de = np.zeros((self.n_inst, 20, 20))
+        e = np.zeros(self.n_inst)
+        check(lib().remc_energy_adjoint(self._h, _ptr(f, C.c_float), _ptr(ft, C.c_double),
+                                        _ptr(dl, C.c_double), _ptr(dx, C.c_double),
+                                        _ptr(de, C.c_double), _ptr(e, C.c_double)))
+        return {"forces": f, "mol_force_torque": ft, "dE_dlambda": dl, "dE_dxi": dx,
+                "dE_deps": de, "energy": e}
+
+    def energy_full_async(self) -> None:
+        """Enqueue the full energy without reading it back."""
+        check(lib().remc_energy_full(self._h, None))
+
+    def adjoint_kernels(self) -> None:
+        """Run the adjoint without copying its outputs back."""
+        check(lib().remc_energy_adjoint(self._h, None, None, None, None, None, None))
+
     def noncrowder_energies(self) -> np.ndarray:
         out = np.zeros(self.n_inst, np.float64)
         check(lib().remc_get_noncrowder_energies(self._h, _ptr(out, C.c_double)))
