@@ -741,12 +741,20 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     const int ta = bead_type(pi.w), mi = ivalid ? bead_mol(pi.w) : -1;
     const bool a_crowd = ta >= kNumAmino;
     float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
-    for (int jj = 0; jj < jn; ++jj) {  // uniform trip count: the j force is warp-reduced
-      const float4 pj = s_j[jj];
-      const int tb = bead_type(pj.w);
-      const bool valid = ivalid && (W.ti != W.tj || jj > tid) && bead_mol(pj.w) != mi;
-      float gx = 0.f, gy = 0.f, gz = 0.f;
-      if (valid) {
+    // j beads in groups of 8: each lane computes its pair with all 8, then a
+    // recursive-halving transpose-reduce sums the 8 j forces over the warp
+    // (27 shuffles for 8 x 3 components instead of 120 for per-j trees)
+    for (int jg = 0; jg < jn; jg += 8) {  // uniform trip count
+      float g[8][3];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        g[q][0] = g[q][1] = g[q][2] = 0.0f;
+        const int jj = jg + q;
+        if (jj >= jn) continue;
+        const float4 pj = s_j[jj];
+        const int tb = bead_type(pj.w);
+        const bool valid = ivalid && (W.ti != W.tj || jj > tid) && bead_mol(pj.w) != mi;
+        if (!valid) continue;
         const float dx = min_image(pi.x - pj.x, box, invbox);
         const float dy = min_image(pi.y - pj.y, box, invbox);
         const float dz = min_image(pi.z - pj.z, box, invbox);
@@ -758,21 +766,21 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
         if (a_crowd || tb >= kNumAmino) {
           const float i6 = rinv2 * rinv2 * rinv2;
           float e = T.x * i6;
-          float p = 6.0f;
+          float pw = 6.0f;
           if (K.crowder_mode) {
             e *= i6;
-            p = 12.0f;
+            pw = 12.0f;
           }
           if (!(r2 < T.z)) e = 0.0f;
           acc_e += e;
-          f = p * e * rinv2;
+          f = pw * e * rinv2;
         } else {
           const float s2 = T.y * rinv2;
           const float s6 = s2 * s2 * s2;
-          const float g = fmaf(-s6, s6, s6);           // s6 (1 - s6)
-          float lj = T.x * g;
+          const float gg = fmaf(-s6, s6, s6);           // s6 (1 - s6)
+          float lj = T.x * gg;
           float dlj = 6.0f * T.x * s6 * fmaf(-2.0f, s6, 1.0f) * rinv2;  // -(dLJ/dr)/r
-          float dg = 4.0f * g;                          // d e_LJ / d eps per c_lj
+          float dg = 4.0f * gg;                         // d e_LJ / d eps per c_lj
           if (r2 < T.z) {
             lj = fmaf(0.5f, T.x, -lj);
             dlj = -dlj;
@@ -781,27 +789,57 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
           const float r = r2 * rinv;
           const float dh = T.w * fast_ex2(r * K.c_xi) * rinv;
           acc_e += lj + dh;
-          acc_x += dh * r;                               // * 1/Xi^2 below
+          acc_x += dh * r;                              // * 1/Xi^2 below
           f = dlj + dh * (C.inv_xi + rinv) * rinv;
           if (ta < kNumAmino && tb < kNumAmino) atomicAdd(&s_G[ta * kNumAmino + tb], dg * C.c_lj);
         }
-        gx = f * dx;
-        gy = f * dy;
-        gz = f * dz;
+        const float gx = f * dx, gy = f * dy, gz = f * dz;
         fx += gx;
         fy += gy;
         fz += gz;
+        g[q][0] = gx;
+        g[q][1] = gy;
+        g[q][2] = gz;
       }
-      // force on j = -(sum over this warp's i of the force on i from j)
-      for (int off = 16; off > 0; off >>= 1) {
-        gx += __shfl_down_sync(0xffffffffu, gx, off);
-        gy += __shfl_down_sync(0xffffffffu, gy, off);
-        gz += __shfl_down_sync(0xffffffffu, gz, off);
+      // level 1 (lane bit 4): keep j 0-3 or 4-7
+      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+      float h4[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float keep = b4 ? g[q + 4][c] : g[q][c];
+          const float send = b4 ? g[q][c] : g[q + 4][c];
+          h4[q][c] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+      // level 2 (bit 3): keep 2 of the 4
+      float h2[2][3];
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float keep = b3 ? h4[q + 2][c] : h4[q][c];
+          const float send = b3 ? h4[q][c] : h4[q + 2][c];
+          h2[q][c] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+      // level 3 (bit 2): keep 1, then sum the remaining two lane bits
+      float h1[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float keep = b2 ? h2[1][c] : h2[0][c];
+        const float send = b2 ? h2[0][c] : h2[1][c];
+        h1[c] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 2);
+        h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 1);
       }
-      if (lane == 0) {
-        s_fj[warp][jj][0] -= gx;
-        s_fj[warp][jj][1] -= gy;
-        s_fj[warp][jj][2] -= gz;
+      if ((lane & 3) == 0) {
+        const int q = (b4 ? 4 : 0) + (b3 ? 2 : 0) + (b2 ? 1 : 0);
+        if (jg + q < jn) {
+          // force on j = -(sum of the forces this warp's i beads feel from j)
+          s_fj[warp][jg + q][0] -= h1[0];
+          s_fj[warp][jg + q][1] -= h1[1];
+          s_fj[warp][jg + q][2] -= h1[2];
+        }
       }
     }
     double de = warp_sum((double)acc_e), dxv = warp_sum((double)acc_x);
