@@ -11,12 +11,14 @@ resident in HBM. `e2e` = the same metric through the C ABI with host buffers:
 every step uploads the full replica state from host memory, runs one block and
 reads state and energies back. Multi-GPU runs are weak scaling: each rank
 advances its own independent batch (a different seed), with no collective on
-the data path.
+the data path; the only collectives reduce the timings (max over ranks) and
+the pair-evaluation counts (sum) after the timed region.
 
---impl reference times the reference's own CPU engine (oracle/_ref/
-REMCDockingCPU, compiled from the reference sources) on bounded samples of
-the same workload, written in the reference's config/PDB formats, with all
-host threads.
+--impl reference times the reference's own CPU engine (Replica::MCSearch,
+compiled from the reference sources into oracle/_ref) on bounded samples of
+the same workload, with all host threads. The reference executable cannot
+load more than 30 molecules (a double free in Replica::loadMolecule), so its
+replicas are built and driven through the harness in oracle/_ref.
 """
 from __future__ import annotations
 
@@ -62,6 +64,29 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MC steps of the per-replica-launch comparison sample")
     return ap.parse_args()
+
+
+# ---------------------------------------------------------------- ranks
+def rank_seed(seed: int, rank: int) -> int:
+    """Workload seed of one rank: every rank generates its own batch."""
+    return seed + 1000 * rank
+
+
+def reduce_over_ranks(times, counts, world: int, device="cpu"):
+    """Max over ranks of each per-rank time and sum of each per-rank count.
+    Every rank calls this with lists of the same lengths at the same point,
+    so all ranks issue the same two collectives in the same order."""
+    if world == 1:
+        return [float(x) for x in times], [float(x) for x in counts]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x) for x in times], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if not counts:
+        return t.tolist(), []
+    c = torch.tensor([float(x) for x in counts], dtype=torch.float64, device=device)
+    dist.all_reduce(c)
+    return t.tolist(), c.tolist()
 
 
 # ---------------------------------------------------------------- clocks
@@ -178,7 +203,7 @@ def main():
     from remcdockingsimulator_b200 import synth
     from remcdockingsimulator_b200.engine import Engine
 
-    w = synth.WORKLOADS[args.workload](args.seed + 1000 * rank)
+    w = synth.WORKLOADS[args.workload](rank_seed(args.seed, rank))
     eng = Engine(w.systems, w.n_replicas, w.params)
     eng.set_replica_params(w.ladders, np.full(len(w.systems), w.translate_step, np.float32),
                            np.full(len(w.systems), w.rotate_step))
@@ -223,21 +248,10 @@ def main():
     clk = clocks.stop()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     ev_res, ev_crowd = eng.pair_evaluations()
-    t_local = ms / 1000.0
-    t_max = t_local
-    if world > 1:
-        t = torch.tensor([t_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    replica_steps = n_inst * B * args.steps * world
+    (t_max,), (pair_evals_all, inst_all) = reduce_over_ranks(
+        [ms / 1000.0], [ev_res + ev_crowd, n_inst], world, "cuda")
+    replica_steps = inst_all * B * args.steps
     value = replica_steps / t_max
-    pair_evals = (ev_res + ev_crowd)
-    if world > 1:
-        t = torch.tensor([float(pair_evals)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t)
-        pair_evals_all = float(t.item())
-    else:
-        pair_evals_all = float(pair_evals)
 
     # ---- roofline of the dominant kernel (the persistent sweep), timed alone
     eng.reset_counters()
@@ -291,8 +305,9 @@ def main():
         with torch.cuda.stream(stream):
             pe.record(stream)
         eng.sync()
-        p_ms = ps.elapsed_time(pe)
-        plain_rate = n_inst * args.plain_steps / (p_ms / 1000.0) * world
+        (p_s,), _ = reduce_over_ranks([ps.elapsed_time(pe) / 1000.0], [], world, "cuda")
+        p_ms = p_s * 1000.0
+        plain_rate = inst_all * args.plain_steps / (p_ms / 1000.0)
         plain = {"value": plain_rate, "unit": "replica-steps/s", "steps": args.plain_steps,
                  "launches": n_inst * args.plain_steps,
                  "batched_over_plain": value / plain_rate}
@@ -311,14 +326,10 @@ def main():
         for dst, src in zip(host, st2):
             dst[...] = src
     eng.sync()
-    t_e2e = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    (t_e2e,), _ = reduce_over_ranks([time.perf_counter() - t0], [], world, "cuda")
     h2d = sum(a.nbytes for a in host)
     d2h = h2d + en.nbytes
-    e2e = {"value": n_inst * B * e2e_steps * world / t_e2e, "unit": "replica-steps/s",
+    e2e = {"value": inst_all * B * e2e_steps / t_e2e, "unit": "replica-steps/s",
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
            "path": "remc_upload_state + remc_run + remc_download_state + remc_get_energies"}
 
@@ -326,7 +337,7 @@ def main():
     # crowded system (all replicas of one system, decorrelated by a sweep)
     adjoint = None
     if args.adjoint_snapshots > 0:
-        wa = synth.crowded(args.seed + 7 + 1000 * rank)
+        wa = synth.crowded(rank_seed(args.seed + 7, rank))
         ea = Engine(wa.systems, [args.adjoint_snapshots], wa.params)
         ea.set_replica_params([np.linspace(290, 480, args.adjoint_snapshots).astype(np.float32)],
                               [wa.translate_step], [wa.rotate_step])
@@ -360,7 +371,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, args.seed)
 
-    gpu_launches = args.steps * 3  # per graph replay: sweep, exchange, counter advance
+    # per timed step: ctrl_set_kernel (remc_run) + the graph's proposal_kernel,
+    # sweep_kernel, exchange_kernel and ctrl_advance_kernel
+    gpu_launches = args.steps * 5
     if rank == 0:
         line = {
             "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",

@@ -280,6 +280,13 @@ class Engine:
         return {"forces": f, "mol_force_torque": ft, "dE_dlambda": dl, "dE_dxi": dx,
                 "dE_deps": de, "energy": e}
 
+    def dE_dlambda(self) -> np.ndarray:
+        """dE/dlambda of every instance only (no forces copied back)."""
+        dl = np.zeros(self.n_inst)
+        check(lib().remc_energy_adjoint(self._h, None, None, _ptr(dl, C.c_double), None, None,
+                                        None))
+        return dl
+
     def energy_full_async(self) -> None:
         """Enqueue the full energy without reading it back."""
         check(lib().remc_energy_full(self._h, None))

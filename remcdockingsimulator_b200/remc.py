@@ -64,6 +64,7 @@ class Args:
     nosim: bool = False
     resume: str = ""
     seed: Optional[int] = None
+    sensitivity: bool = False
     output_dir: str = "output"
     data_dir: str = "data"
     files: List[Tuple[str, bool]] = dataclasses.field(default_factory=list)
@@ -134,6 +135,9 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
         elif t == "--seed":
             a.seed = int(val())
             i += 2
+        elif t == "--sensitivity":
+            a.sensitivity = True
+            i += 1
         elif t == "--output-dir":
             a.output_dir = val()
             i += 2
@@ -149,7 +153,7 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
 
 USAGE = ("Usage: python -m remcdockingsimulator_b200 -f <filename> [-c] [-h] [-v] [-q] [-t x] "
          "[-s x] [-g x] [-m x] [-e x] [-r x] [-o x] [-b x] [-t0 x] [-t1 x] [-bx x] "
-         "[--seed x] [--output-dir d] [--data-dir d]")
+         "[--seed x] [--sensitivity] [--output-dir d] [--data-dir d]")
 
 _PLACE = re.compile(r"^([tp])\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*"
                     r"r\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*(\S+)")
@@ -326,6 +330,8 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
         pend_rej = np.zeros(R, np.int64)
         last = [np.zeros(R, np.int64) for _ in range(5)]
         total_ex = total_tests = 0
+        sens = np.zeros((R, 4))  # per temperature: n, sum B, sum X, sum B X (X = dE/dlambda)
+        has_crowders = system.n_chains < system.n_mol
         t0 = time.perf_counter()
         step0 = 0
         for steps in range(1, a.resteps + 1):
@@ -352,6 +358,15 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
                         p[6]))
             if dropped:
                 log("-!- %d bound conformations did not fit the record buffer" % dropped)
+            if a.sensitivity:
+                # fluctuation estimate of d<bound>/dlambda from block-end states
+                en = eng.energies()
+                enc = en + eng.noncrowder_energies() if has_crowders else en
+                X = eng.dE_dlambda()
+                tmap = eng.temperature_map()
+                for slot in range(R):
+                    B = 1.0 if enc[slot] < float(BOUND_ENERGY) else 0.0
+                    sens[tmap[slot]] += (1.0, B, X[slot], B * X[slot])
             if steps == a.resteps:
                 break
             tos = eng.temperature_map()
@@ -414,13 +429,38 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
         files.fb.write("\n")
         files.ar.write("\n")
         files.close()
+        sensitivity = None
+        if a.sensitivity:
+            sensitivity = sensitivity_estimates(ladder, sens)
+            with open(files.base + "_sensitivity", "w") as fh:
+                fh.write("# temperature samples <B> <dE/dlambda> d<B>/dlambda "
+                         "(= -beta (<B X> - <B><X>), X = dE/dlambda, kcal/mol)\n")
+                for T, n, b, x, d in sensitivity:
+                    fh.write("%0.1f %d %.6f %.6f %.6e\n" % (T, n, b, x, d))
         energies = eng.energies()
         log("Simulation: %10.5f ms  (%d exchanges)" % (elapsed * 1000.0, a.resteps))
         return {"elapsed_s": elapsed, "replica_steps": R * per * a.resteps, "e0": e0,
+                "sensitivity": sensitivity,
                 "energies": energies, "temperature_of_slot": tos, "files": files.base,
                 "fraction_bound": _fmt_ratio(tot_bound.sum(), tot_samples.sum())}
     finally:
         eng.close()
+
+
+def sensitivity_estimates(ladder: np.ndarray, sums: np.ndarray):
+    """Fluctuation formula d<B>/dtheta = -beta (<B X> - <B><X>), X = dE/dtheta,
+    beta = 4184 / (R T) per kcal/mol, from per-temperature sums
+    (n, sum B, sum X, sum B X). Returns (T, n, <B>, <X>, d<B>/dtheta) rows."""
+    out = []
+    for t, T in enumerate(ladder):
+        n, sb, sx, sbx = sums[t]
+        if n == 0:
+            out.append((float(T), 0, float("nan"), float("nan"), float("nan")))
+            continue
+        beta = 4184.0 / (float(np.float32(8.314472)) * float(T))
+        mb, mx, mbx = sb / n, sx / n, sbx / n
+        out.append((float(T), int(n), mb, mx, -beta * (mbx - mb * mx)))
+    return out
 
 
 def check_mode(data_dir: str, table: AminoAcidTable, log=print) -> List[Tuple[float, float]]:

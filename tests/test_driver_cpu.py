@@ -82,3 +82,17 @@ def test_pdb_reader_repeats_last_bead_after_final_newline(tmp_path, built_lib):
     p.write_text("ATOM      1  CA  ALA A   1       1.000   2.000   3.000  1.00  1.00\nEND\n")
     types, xyz = read_pdb_ca(str(p), table)
     assert len(types) == 1
+
+
+def test_sensitivity_estimator(built_lib):
+    """The fluctuation formula on synthetic samples: B = 1{X < 0} with X
+    Gaussian; -beta(<BX> - <B><X>) = beta sigma phi(0) for zero-mean X."""
+    from remcdockingsimulator_b200 import remc
+    rng = np.random.default_rng(0)
+    X = rng.normal(0.0, 2.0, size=200000)
+    B = (X < 0).astype(float)
+    sums = np.array([[len(X), B.sum(), X.sum(), (B * X).sum()]])
+    (T, n, mb, mx, d), = remc.sensitivity_estimates(np.array([300.0]), sums)
+    beta = 4184.0 / (8.314472 * 300.0)
+    assert abs(mb - 0.5) < 0.01
+    assert abs(d - beta * 2.0 / np.sqrt(2 * np.pi)) < 0.02 * beta

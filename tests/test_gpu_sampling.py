@@ -82,6 +82,7 @@ def test_driver_writes_reference_output_files(tmp_path, built_lib):
     mols = remc.load_config(a, table, log=lambda *_: None)
     remc.parse_cli(["-f", cfg, "-r", "6"], a)  # flags override the file, as main() does
     a.sample_after = 0
+    a.sensitivity = True
     remc.write_file_index(a)
     from remcdockingsimulator_b200.model import System
     summary = remc.simulate(a, System(mols, a.bound, table), log=lambda *_: None)
@@ -97,3 +98,9 @@ def test_driver_writes_reference_output_files(tmp_path, built_lib):
     idx = open(os.path.join(d, "output", "synth_repulsive_4242_fileindex")).read().splitlines()
     assert idx[0] == "index molecule_file_path crowder(Y/N)" and idx[-1].endswith(" Y")
     assert summary["replica_steps"] == 6 * 400
+    # fluctuation sensitivities: one row per temperature, one sample per
+    # replica per block
+    sens = open(base + "_sensitivity").read().splitlines()[1:]
+    assert len(sens) == 6
+    assert sum(int(l.split()[1]) for l in sens) == 6 * 4
+    assert all(np.isfinite(float(l.split()[4])) for l in sens if int(l.split()[1]) > 0)
