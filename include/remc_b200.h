@@ -126,6 +126,13 @@ int remc_exchange(remc_handle* h, uint64_t seed, uint32_t round, int offset);
 
 /* temp_of_slot[n_inst]: temperature index held by each instance's slot. */
 int remc_get_temperature_map(remc_handle* h, int* temp_of_slot);
+/* Checkpoint restore (no reference counterpart; the reference's resume path,
+ * main.cpp:119-160, re-derives conformations from rounded text): set the
+ * temperature index held by every slot (a permutation of 0..R-1 within each
+ * system), and the running energy and chain-chain energy of every instance
+ * (noncrowder may be NULL), so that a restored run continues bit for bit. */
+int remc_set_temperature_map(remc_handle* h, const int* temp_of_slot);
+int remc_set_energies(remc_handle* h, const double* energy, const double* noncrowder);
 /* Per-instance move counters since the last reset: accepted with dE < 0,
  * accepted by the Boltzmann test, rejected; exchange counters per system. */
 int remc_get_counters(remc_handle* h, int* accept, int* acceptA, int* reject);

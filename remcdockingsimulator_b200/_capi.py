@@ -74,6 +74,8 @@ _SIGS = {
     "remc_sweep_plain": (C.c_int, [P, C.c_int, C.c_uint64, C.c_uint32]),
     "remc_exchange": (C.c_int, [P, C.c_uint64, C.c_uint32, C.c_int]),
     "remc_get_temperature_map": (C.c_int, [P, PI]),
+    "remc_set_temperature_map": (C.c_int, [P, PI]),
+    "remc_set_energies": (C.c_int, [P, PD, PD]),
     "remc_get_counters": (C.c_int, [P, PI, PI, PI]),
     "remc_reset_counters": (C.c_int, [P]),
     "remc_delta_energy": (C.c_int, [P, C.c_int, C.c_int, PF, PD]),

@@ -1811,6 +1811,43 @@ int remc_get_temperature_map(remc_handle* h, int* temp_of_slot) {
   return REMC_OK;
 }
 
+int remc_set_temperature_map(remc_handle* h, const int* temp_of_slot) {
+  if (!h || !temp_of_slot) return set_error(REMC_ERR_INVALID, "null argument");
+  if (!h->replica_params_set) return set_error(REMC_ERR_STATE, "replica parameters not set");
+  std::vector<int> slot_of(h->n_inst, -1);
+  for (int s = 0; s < h->n_sys; ++s) {
+    const SysDev& S = h->h_sys[s];
+    for (int k = 0; k < S.n_rep; ++k) {
+      const int t = temp_of_slot[S.inst0 + k];
+      if (t < 0 || t >= S.n_rep || slot_of[S.inst0 + t] >= 0)
+        return set_error(REMC_ERR_INVALID,
+                         "system %d: temperature map is not a permutation of 0..%d", s,
+                         S.n_rep - 1);
+      slot_of[S.inst0 + t] = k;
+    }
+  }
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_temp_idx, temp_of_slot, sizeof(int) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_slot_of_temp, slot_of.data(), sizeof(int) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
+int remc_set_energies(remc_handle* h, const double* energy, const double* noncrowder) {
+  if (!h || !energy) return set_error(REMC_ERR_INVALID, "null argument");
+  for (int g = 0; g < h->n_inst; ++g)
+    if (!std::isfinite(energy[g]) || (noncrowder && !std::isfinite(noncrowder[g])))
+      return set_error(REMC_ERR_NUMERIC, "instance %d: non-finite energy", g);
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_energy, energy, sizeof(double) * h->n_inst,
+                                cudaMemcpyHostToDevice, h->stream));
+  if (noncrowder)
+    REMC_CUDA_TRY(cudaMemcpyAsync(h->d_ecc, noncrowder, sizeof(double) * h->n_inst,
+                                  cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return REMC_OK;
+}
+
 int remc_get_counters(remc_handle* h, int* accept, int* acceptA, int* reject) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (accept)

@@ -221,6 +221,17 @@ class Engine:
         check(lib().remc_get_temperature_map(self._h, _ptr(out, C.c_int)))
         return out
 
+    def set_temperature_map(self, temp_of_slot) -> None:
+        t = np.ascontiguousarray(temp_of_slot, np.int32)
+        check(lib().remc_set_temperature_map(self._h, _ptr(t, C.c_int)))
+
+    def set_energies(self, energy, noncrowder=None) -> None:
+        """Restore the running energies (checkpoint resume)."""
+        e = np.ascontiguousarray(energy, np.float64)
+        c = None if noncrowder is None else np.ascontiguousarray(noncrowder, np.float64)
+        check(lib().remc_set_energies(self._h, _ptr(e, C.c_double),
+                                      None if c is None else _ptr(c, C.c_double)))
+
     def counters(self):
         a = np.zeros(self.n_inst, np.int32)
         b = np.zeros(self.n_inst, np.int32)

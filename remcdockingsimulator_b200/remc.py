@@ -65,6 +65,8 @@ class Args:
     resume: str = ""
     seed: Optional[int] = None
     sensitivity: bool = False
+    checkpoint_every: int = 0  # MC steps between checkpoints (0: off)
+    checkpoint_dir: str = "checkpoints"
     output_dir: str = "output"
     data_dir: str = "data"
     files: List[Tuple[str, bool]] = dataclasses.field(default_factory=list)
@@ -135,6 +137,12 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
         elif t == "--seed":
             a.seed = int(val())
             i += 2
+        elif t == "--checkpoint-every":
+            a.checkpoint_every = int(val())
+            i += 2
+        elif t == "--checkpoint-dir":
+            a.checkpoint_dir = val()
+            i += 2
         elif t == "--sensitivity":
             a.sensitivity = True
             i += 1
@@ -153,7 +161,8 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
 
 USAGE = ("Usage: python -m remcdockingsimulator_b200 -f <filename> [-c] [-h] [-v] [-q] [-t x] "
          "[-s x] [-g x] [-m x] [-e x] [-r x] [-o x] [-b x] [-t0 x] [-t1 x] [-bx x] "
-         "[--seed x] [--sensitivity] [--output-dir d] [--data-dir d]")
+         "[-z checkpoint] [--seed x] [--sensitivity] [--checkpoint-every steps] "
+         "[--checkpoint-dir d] [--output-dir d] [--data-dir d]")
 
 _PLACE = re.compile(r"^([tp])\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*"
                     r"r\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*(\S+)")
@@ -262,13 +271,16 @@ def _fmt_ratio(num: float, den: float) -> float:
 class OutputFiles:
     """The four sampling files (main.cpp:634-713) plus the file index."""
 
-    def __init__(self, a: Args, ladder: np.ndarray):
+    def __init__(self, a: Args, ladder: np.ndarray, header: bool = True):
         os.makedirs(a.output_dir, exist_ok=True)
         base = os.path.join(a.output_dir, "%s_%d" % (a.prefix, a.pid))
         self.fb = open(base + "_fractionBound", "a")
         self.bc = open(base + "_boundconformations", "a")
         self.ar = open(base + "_acceptance_ratios", "a")
         self.ex = open(base + "_exchange_freq", "a")
+        self.base = base
+        if not header:  # a resumed run appends to the files of the run it continues
+            return
         self.fb.write("# Fraction Bound\n#Iteration InstantaniousAve CumulativeAve\n")
         self.bc.write("# iteration; complex free energy (replica free energy); temperature;\n"
                       "# molecule: rotation(w,x,y,z) position(x,y,z) 1 line per other molecule "
@@ -282,11 +294,101 @@ class OutputFiles:
             self.ar.write("%0.1fKi %0.1fKc " % (T, T))
         self.fb.write("\t\n")
         self.ar.write("\n")
-        self.base = base
+
+    def flush(self):
+        for f in (self.fb, self.bc, self.ar, self.ex):
+            f.flush()
 
     def close(self):
         for f in (self.fb, self.bc, self.ar, self.ex):
             f.close()
+
+
+# ------------------------------------------------------------------ checkpoints
+CHECKPOINT_FREQUENCY = 10000  # definitions.h:116, MC steps between checkpoints
+
+_CK_PARAMS = ("# threads, streams, gpus, MCsteps, RESteps, sampleFrequency, sampleStartsAfter,"
+              "nonCrowders, temperatureMin, temperatureMax, currentStep")
+_CK_STATS = ("stats: accept, acceptA, reject, totalAcceptReject, totalAccept, boundSamples, "
+             "samplesSinceLastExchange, totalBoundSamples, totalSamples")
+# driver accumulators saved with the engine state
+_CK_ARRAYS = ("tot_bound", "tot_samples", "tot_acc", "tot_all", "pend_bound", "pend_samples",
+              "pend_acc", "pend_accA", "pend_rej", "sens")
+
+
+def checkpoint_path(a: Args) -> str:
+    return os.path.join(a.checkpoint_dir, "%s_%d" % (a.prefix, a.pid))
+
+
+def save_simulation(a: Args, path: str, blocks: int, seed: int, state, energies, ecc, tmap,
+                    acc: dict, total_ex: int, total_tests: int) -> None:
+    """saveSimulation (main.cpp:89-117): the reference's text layout (config
+    file, prefix_pid, pid, run parameters with the current step, molecule and
+    replica counts, then per replica slot one line per molecule with its
+    position and rotation quaternion at %.7f and one statistics line), plus a
+    line naming an .npz file with the exact engine state (coordinates, running
+    energies, temperature map), the Philox seed and the driver's accumulators,
+    from which a resumed run continues bit for bit."""
+    pos, rel, cen, quat = state
+    R = len(tmap)
+    n_mol = cen.shape[0] // R
+    per = a.mcsteps // a.resteps
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    npz = path + ".state.npz"
+    tmp = npz + ".tmp.npz"
+    np.savez(tmp, pos=pos, rel=rel, centre=cen, quat=quat, energies=energies, ecc=ecc,
+             tmap=tmap, seed=np.uint64(seed), blocks=np.int64(blocks),
+             total_ex=np.int64(total_ex), total_tests=np.int64(total_tests),
+             **{k: acc[k] for k in _CK_ARRAYS})
+    os.replace(tmp, npz)
+    lines = ["#Saved simulation state file, prependage string, original pid", a.file,
+             "%s_%d" % (a.prefix, a.pid), "%d" % a.pid, _CK_PARAMS,
+             "%d %d %d %d %d %d %d %d %f %f %d" % (a.threads, a.streams, a.gpus, a.mcsteps,
+                                                   a.resteps, a.sample_frequency, a.sample_after,
+                                                   a.noncrowders, a.tmin, a.tmax, per * blocks),
+             "#molecules", "%d" % n_mol, "#replicas", "%d" % R]
+    for r in range(R):
+        t = int(tmap[r])
+        lines.append("#replica %d, molecules: x,y,z translation. w,x,y,z rotation quaternion" % r)
+        for m in range(n_mol):
+            c, q = cen[r * n_mol + m], quat[r * n_mol + m]
+            lines.append("%.7f %.7f %.7f %.7f %.7f %.7f %.7f" % (c[0], c[1], c[2], q[0], q[1],
+                                                                 q[2], q[3]))
+        lines.append("#replica %d, %s" % (r, _CK_STATS))
+        lines.append("%d %d %d %d %d %d %d %d %d" % (
+            acc["pend_acc"][r], acc["pend_accA"][r], acc["pend_rej"][r], acc["tot_all"][t],
+            acc["tot_acc"][t], acc["pend_bound"][r], acc["pend_samples"][r], acc["tot_bound"][t],
+            acc["tot_samples"][t]))
+    lines.append("#exact state %s" % os.path.basename(npz))
+    tmp = path + ".tmp"
+    with open(tmp, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    os.replace(tmp, path)
+
+
+def read_checkpoint_header(path: str) -> dict:
+    """The fields of a saved simulation that select the run to resume: the
+    config file, prefix_pid, pid and the run parameters line."""
+    with open(path) as fh:
+        lines = [ln.rstrip("\n") for ln in fh]
+    if len(lines) < 6 or not lines[0].startswith("#Saved simulation state"):
+        raise ArgError("%s is not a saved simulation" % path)
+    vals = lines[5].split()
+    exact = [ln.split(None, 2)[2] for ln in lines if ln.startswith("#exact state ")]
+    return {"file": lines[1], "prefix_pid": lines[2], "pid": int(lines[3]),
+            "mcsteps": int(vals[3]), "resteps": int(vals[4]), "current_step": int(vals[10]),
+            "replicas": int(lines[9]), "n_mol": int(lines[7]),
+            "exact": os.path.join(os.path.dirname(os.path.abspath(path)), exact[0])
+            if exact else None}
+
+
+def load_simulation(path: str) -> dict:
+    hdr = read_checkpoint_header(path)
+    if hdr["exact"] is None or not os.path.exists(hdr["exact"]):
+        raise ArgError("%s: exact state file missing" % path)
+    with np.load(hdr["exact"]) as z:
+        hdr.update({k: z[k] for k in z.files})
+    return hdr
 
 
 def write_file_index(a: Args) -> None:
@@ -297,8 +399,12 @@ def write_file_index(a: Args) -> None:
             fh.write("%2d %s %s\n" % (i, path, "Y" if crowd else "N"))
 
 
-def simulate(a: Args, system: System, params=None, log=print) -> dict:
-    """REMCSimulation on the GPU engine. Returns summary statistics."""
+def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None) -> dict:
+    """REMCSimulation on the GPU engine. Returns summary statistics. With
+    a.resume set, continues the run saved in that checkpoint; with
+    a.checkpoint_every > 0, saves a checkpoint after every exchange round that
+    completes that many MC steps (on_checkpoint(path, blocks) is called after
+    each save)."""
     from .engine import Engine, make_params
 
     R = a.replicas
@@ -307,7 +413,16 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
     eng = Engine([system], R, params if params is not None else make_params())
     try:
         eng.set_replica_params([ladder], tsteps, rsteps)
-        e0 = eng.energy_full()
+        ck = load_simulation(a.resume) if a.resume else None
+        if ck is None:
+            e0 = eng.energy_full()
+        else:
+            if int(ck["replicas"]) != R or ck["pos"].shape[0] != R * system.n_beads:
+                raise ArgError("checkpoint does not match this configuration")
+            eng.upload_state(ck["pos"], ck["rel"], ck["centre"], ck["quat"])
+            eng.set_temperature_map(ck["tmap"])
+            eng.set_energies(ck["energies"], ck["ecc"])
+            e0 = np.array(ck["energies"], np.float64)
         per = a.mcsteps // a.resteps
         if per <= 0:
             raise ArgError("mcsteps must be at least resteps")
@@ -315,8 +430,10 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
         n_mol = system.n_mol
         max_rec = max(1, R * max(1, per // max(f, 1)))
         eng.set_sampling(f, a.sample_after, float(BOUND_ENERGY), max_rec, max_rec * n_mol)
-        files = OutputFiles(a, ladder)
+        files = OutputFiles(a, ladder, header=ck is None)
         seed = a.seed if a.seed is not None else int(time.time())
+        if ck is not None:
+            seed = int(ck["seed"])
         # host mirror of the reference's per-replica statistics: slot counters
         # since the last report, cumulative totals that follow the temperature
         tot_bound = np.zeros(R, np.int64)
@@ -332,9 +449,23 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
         total_ex = total_tests = 0
         sens = np.zeros((R, 4))  # per temperature: n, sum B, sum X, sum B X (X = dE/dlambda)
         has_crowders = system.n_chains < system.n_mol
+        first_block = 1
+        if ck is not None:
+            for name, arr in (("tot_bound", tot_bound), ("tot_samples", tot_samples),
+                              ("tot_acc", tot_acc), ("tot_all", tot_all),
+                              ("pend_bound", pend_bound), ("pend_samples", pend_samples),
+                              ("pend_acc", pend_acc), ("pend_accA", pend_accA),
+                              ("pend_rej", pend_rej), ("sens", sens)):
+                arr[...] = ck[name]
+            total_ex, total_tests = int(ck["total_ex"]), int(ck["total_tests"])
+            first_block = int(ck["blocks"]) + 1
+            log("Resuming after exchange round %d (step %d)" % (first_block - 1,
+                                                                per * (first_block - 1)))
+        ck_every = a.checkpoint_every
+        until_ck = ck_every
         t0 = time.perf_counter()
-        step0 = 0
-        for steps in range(1, a.resteps + 1):
+        step0 = per * (first_block - 1)
+        for steps in range(first_block, a.resteps + 1):
             eng.sweep(per, seed, step0)
             step0 += per
             n_s, n_b = eng.sample_counters()
@@ -410,6 +541,22 @@ def simulate(a: Args, system: System, params=None, log=print) -> dict:
             files.ex.write("%10d %6.4f %6.4f\n" % (steps, _fmt_ratio(total_ex, total_tests),
                                                    _fmt_ratio(exchanges, tests)))
             log("Replica Exchange step %d of %d complete" % (steps, a.resteps))
+            if ck_every > 0:
+                until_ck -= per
+                if until_ck <= 0:
+                    until_ck = ck_every
+                    files.flush()
+                    path = checkpoint_path(a)
+                    acc_state = {"tot_bound": tot_bound, "tot_samples": tot_samples,
+                                 "tot_acc": tot_acc, "tot_all": tot_all,
+                                 "pend_bound": pend_bound, "pend_samples": pend_samples,
+                                 "pend_acc": pend_acc, "pend_accA": pend_accA,
+                                 "pend_rej": pend_rej, "sens": sens}
+                    save_simulation(a, path, steps, seed, eng.download_state(), eng.energies(),
+                                    eng.noncrowder_energies(), eng.temperature_map(), acc_state,
+                                    total_ex, total_tests)
+                    if on_checkpoint is not None:
+                        on_checkpoint(path, steps)
         eng.sync()
         elapsed = time.perf_counter() - t0
         # final lines (main.cpp:1509-1538)
@@ -499,6 +646,11 @@ def main(argv: Optional[List[str]] = None) -> int:
         print(e)
         return 0
     a.pid = os.getpid()
+    if a.resume:
+        # getArgs -z (main.cpp:351-368): the config file and pid come from the
+        # checkpoint, so the output files continue under the original name
+        hdr = read_checkpoint_header(a.resume)
+        a.file, a.pid, a.input_file = hdr["file"], hdr["pid"], True
     table = AminoAcidTable.load(os.path.join(a.data_dir, "AminoAcids"))
     table.load_pairs(os.path.join(a.data_dir, "pair_potentials_MJ1996"))
     if a.check:
