@@ -215,7 +215,7 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
  * reference fixes its block size by system size, main.cpp:1746-1747). */
 int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads,
                   int* mol_in_smem, float* best_ms);
-/* Set the sweep schedule directly (threads a multiple of 32, <= 256). */
+/* Set the sweep schedule directly (threads 32, 64, 128 or 256). */
 int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem);
 
 int remc_sync(remc_handle* h);

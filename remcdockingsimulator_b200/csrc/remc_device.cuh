@@ -62,6 +62,7 @@ __device__ __forceinline__ float fast_ex2(float x) {
 struct EnergyConsts {
   float c_xi;        // -log2(e) / Xi: exp(-r/Xi) = ex2(r * c_xi)
   int crowder_mode;  // 0: A r^-6; 1: A r^-12
+  int crowder_cut;   // 1: crowder pairs beyond the cutoff contribute nothing
 };
 
 // Round to nearest, ties to even, on the FMA pipe: adding and subtracting
@@ -98,6 +99,20 @@ __device__ __forceinline__ float pair_energy_r2(float r2, float4 T, bool crowd,
   float r = r2 * rinv;
   float dh = T.w * fast_ex2(r * K.c_xi) * rinv;
   return lj + dh;
+}
+
+// The crowder branch of pair_energy_r2 with the model fixed at compile time
+// (R12: A r^-12, else A r^-6; CUT: zero at r^2 >= cut2). Same operations in
+// the same order, so the same value.
+template <bool R12, bool CUT>
+__device__ __forceinline__ float crowd_energy(float r2, float A, float cut2) {
+  float rinv = fast_rsqrt(r2);
+  float rinv2 = rinv * rinv;
+  float i6 = rinv2 * rinv2 * rinv2;
+  float e = A * i6;
+  if (R12) e *= i6;
+  if (CUT) e = (r2 < cut2) ? e : 0.0f;
+  return e;
 }
 
 __device__ __forceinline__ float pair_r2(float4 a, float4 b, float L, float invL) {

@@ -72,6 +72,7 @@ struct SysDev {
   float box, invbox;
   int translate_only_crowders;
   int n_chain_beads;  // beads of residue type; the rest are crowders
+  int crowd_type;     // the one bead type of every crowder, or -1 (none or mixed)
 };
 
 // Per-step proposal record: everything about step s of one replica that does
@@ -83,9 +84,12 @@ struct StepRec {
   double thr;       // Metropolis threshold -log(u)/beta: accept iff dE < thr
   float t[3];       // translation vector
   int m;            // molecule
-  int rotate;       // 1 rotation, 0 translation
-  int crowd;        // 1 if the molecule is a crowder
+  int m0;           // its first bead
+  int info;         // bits 0-29: its bead count; bit 30: rotation; bit 31: crowder
 };
+constexpr int kRecRotate = 1 << 30;
+constexpr int kRecCrowd = (int)(1u << 31);
+constexpr int kRecCount = kRecRotate - 1;
 static_assert(sizeof(StepRec) == 64, "StepRec layout");
 
 struct ProposalArgs {
@@ -125,13 +129,16 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
   StepRec r;
   r.m = (int)__dmul_rn(u0, (double)S.n_mol);
   const bool crowd = P.mol_role[P.mrole_off[sysid] + r.m] == -1;
-  r.rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
+  const bool rotate = (u1 < 0.5) && !(S.translate_only_crowders && crowd);
+  r.m0 = P.mol_start[S.mstart_off + r.m];
+  r.info = (P.mol_start[S.mstart_off + r.m + 1] - r.m0) | (rotate ? kRecRotate : 0) |
+           (crowd ? kRecCrowd : 0);
   // u < exp(-beta dE)  <=>  dE < -log(u)/beta  (Replica.cpp:451); u = 0 never
   // passes the reference's test, so its threshold is -inf
   const float T = P.ladder[S.inst0 + P.temp_idx[inst]];
   const double beta = 4184.0 / ((double)8.314472f * (double)T);
   r.thr = u5 > 0.0 ? -log(u5) / beta : -INFINITY;
-  if (r.rotate) {
+  if (rotate) {
     step_quaternion(u2, u3, u4, P.rot_cs[2 * inst], P.rot_cs[2 * inst + 1], r.q);
     r.t[0] = r.t[1] = r.t[2] = 0.0f;
   } else {
@@ -142,7 +149,6 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
     r.q[0] = 1.0;
     r.q[1] = r.q[2] = r.q[3] = 0.0;
   }
-  r.crowd = crowd ? 1 : 0;
   P.recs[(size_t)inst * P.rec_stride + s] = r;
 }
 
@@ -210,7 +216,7 @@ constexpr int kRing = 64;  // proposal records held in shared memory (two halves
 // Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
 // mmax molecules, lmax beads per molecule).
 struct SweepSmem {
-  size_t tab, beads, centres, trial_pos, mstart, ring, red, total;
+  size_t tab, beads, centres, trial_pos, ring, red, total;
   static __host__ __device__ size_t take(size_t& off, size_t bytes) {
     size_t o = off;
     off += (bytes + 15) & ~size_t(15);
@@ -225,13 +231,21 @@ struct SweepSmem {
     s.beads = take(off, sizeof(float4) * nmax);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
-    s.mstart = take(off, mol_in_smem ? sizeof(int) * (mmax + 1) : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * 2 * 32);
     s.total = off;
     return s;
   }
 };
+
+// Sum of nw <= 8 FP64 partials in a fixed pairwise order (missing entries add
+// an exact zero); every thread evaluates it and gets the same value.
+__device__ __forceinline__ double tree_sum8(const double* v, int nw) {
+  double a[8];
+#pragma unroll
+  for (int w = 0; w < 8; ++w) a[w] = w < nw ? v[w] : 0.0;
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -251,18 +265,19 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the trial buffer rather than from another thread's not-yet-ordered write.
 // A step of a one-bead molecule therefore costs one barrier; a chain step
 // costs two (trial positions are built by the owners of the chain's beads).
-__global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
+template <bool R12, bool CUT>
+__global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
   float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
   float4* s_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
-  int* s_mstart = reinterpret_cast<int*>(smem_raw + L.mstart);
   StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
 
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tmask = nthr - 1;  // nthr is a power of two
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
   __shared__ int s_next;
   for (int it = 0;; ++it) {
@@ -291,15 +306,12 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
   for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
-  // molecule centres and starts: shared memory, or global memory for the
-  // largest systems (thread 0 writes a centre; others read it only after a
-  // later barrier, which orders global memory within the CTA as well)
+  // molecule centres: shared memory, or global memory for the largest
+  // systems (thread 0 writes a centre; others read it only after a later
+  // barrier, which orders global memory within the CTA as well)
   float4* cent = A.mol_in_smem ? s_cent : A.centre + mol_off;
-  const int* mst = A.mol_in_smem ? s_mstart : A.mol_start + S.mstart_off;
-  if (A.mol_in_smem) {
+  if (A.mol_in_smem)
     for (int i = tid; i < M; i += nthr) s_cent[i] = A.centre[mol_off + i];
-    for (int i = tid; i <= M; i += nthr) s_mstart[i] = A.mol_start[S.mstart_off + i];
-  }
   {
     // first ring fill: records of steps 0..min(kRing, n_steps)-1, 16 B per copy
     const int nrec = min(kRing, n_steps);
@@ -315,10 +327,14 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
   int n_neg = 0, n_boltz = 0, n_rej = 0, n_samp = 0, n_bnd = 0;
   unsigned long long ev_kh = 0, ev_crowd = 0;
   const int ncb = S.n_chain_beads;  // beads [0, ncb) belong to chains
+  const int ctype = S.crowd_type;   // the crowders' one type, or -1
   const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
   int to_sample = A.sample_every;  // steps left in the current sampling chunk
   __shared__ long long s_pose_slot;
   __syncthreads();
+  // centre of the next step's molecule when centres live in global memory
+  float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (n_steps > 0 && !A.mol_in_smem) next_c = cent[s_ring[0].m];
 
   // previous step, known to every thread
   int p_m = -1, p_acc = 0, p_rot = 0, p_n = 0, p_b = 0;
@@ -342,23 +358,24 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
       float t[3];
     } rec;
     rec.m = recs_.m;
-    rec.rotate = recs_.rotate;
-    rec.crowd = recs_.crowd;
+    rec.rotate = (recs_.info & kRecRotate) != 0;
+    rec.crowd = (recs_.info & kRecCrowd) != 0;
     rec.t[0] = recs_.t[0];
     rec.t[1] = recs_.t[1];
     rec.t[2] = recs_.t[2];
     const int m = rec.m;
-    const int m0 = mst[m], n = mst[m + 1] - m0;
+    const int m0 = recs_.m0, n = recs_.info & kRecCount;
     const int b = s & 1;
     const bool same = (m == p_m) && p_acc;  // moved (and accepted) last step
-    // centre of m: the one this step's thread computed last step if m moved then
+    // centre of m: the one this step's thread computed last step if m moved
+    // then, else the one loaded at the end of the previous step
     float c0, c1, c2;
     if (same && !p_rot) {
       c0 = p_nc0;
       c1 = p_nc1;
       c2 = p_nc2;
     } else {
-      const float4 c = cent[m];
+      const float4 c = A.mol_in_smem ? cent[m] : next_c;
       c0 = c.x;
       c1 = c.y;
       c2 = c.z;
@@ -379,7 +396,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
       // trial positions of the chain, built by the owners of its beads
       QuatProducts qp{};
       if (rec.rotate) qp = quat_products(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3]);
-      int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
+      int j = m0 + ((tid - m0) & tmask);
       for (; j < m0 + n; j += nthr) {
         const int k = j - m0;
         const float4 rl = A.rel[bead_off + j];
@@ -396,63 +413,103 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
       __syncthreads();  // trial positions and the previous chain update visible
     }
 
-    // ---- dE over beads j outside the molecule (thread t owns j = t mod T);
-    // for a chain, the part from other chains' beads (j < ncb) is kept apart:
-    // it is the change of the chain-chain energy sample() adds
+    // ---- dE over beads j outside the molecule (thread t owns j = t mod T).
+    // Beads are chains [0, ncb) then crowders [ncb, N); the moved molecule's
+    // own beads [m0, m0 + n) split the range in two. Residue-residue pairs of
+    // a chain move are the change of the chain-chain energy sample() adds.
     double dacc = 0.0, dcc = 0.0;
-    const bool split = !rec.crowd && ncb < N;
     if (!skip) {
-      for (int k = 0; k < n; ++k) {
-        float4 pold, pnew;
-        if (n == 1) {
-          pold = pold1;
-          pnew = pnew1;
-        } else {
-          pold = (same) ? s_tpos[p_b * A.lmax + k] : s_beads[m0 + k];
-          pnew = s_tpos[b * A.lmax + k];
-        }
-        const int ta = bead_type(pold.w);
-        const bool a_crowd = ta >= kNumAmino;
+      const int x0 = m0, x1 = m0 + n;
+      float acc_c = 0.0f, acc_o = 0.0f;
+      if (n == 1) {
+        // one bead (a crowder or a one-residue chain), positions in registers
+        const int ta = bead_type(pold1.w);
         const float4* trow = s_tab + ta * kNT;
-        float acc_c = 0.0f, acc_o = 0.0f;
-        if (split) {
-          // a chain in a crowded system: other chains' beads first (j < ncb)
-          int j = tid;
-          for (; j < ncb; j += nthr) {
-            if (j >= m0 && j < m0 + n) continue;
-            const float4 pj = s_beads[j];
-            const float4 Tj = trow[bead_type(pj.w)];
-            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, false, A.K);
-            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, false, A.K);
-            acc_c += en - eo;
+        for (int part = 0; part < 2; ++part) {
+          const int lo = part ? x1 : 0, hi = part ? N : x0;
+          if (lo >= hi) continue;
+          const int cb = min(hi, ncb);
+          int j = lo + ((tid - lo) & tmask);  // first j >= lo with j = tid (mod T)
+          if (!rec.crowd) {
+            for (; j < cb; j += nthr) {
+              const float4 pj = s_beads[j];
+              const float4 Tj = trow[bead_type(pj.w)];
+              const float en = pair_energy_r2(pair_r2(pnew1, pj, box, invbox), Tj, false, A.K);
+              const float eo = pair_energy_r2(pair_r2(pold1, pj, box, invbox), Tj, false, A.K);
+              acc_c += en - eo;
+            }
+          } else {
+            for (; j < cb; j += nthr) {
+              const float4 pj = s_beads[j];
+              const float4 Tj = trow[bead_type(pj.w)];
+              const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
+              const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pj, box, invbox), Tj.x, Tj.z);
+              acc_o += en - eo;
+            }
           }
-          for (; j < N; j += nthr) {
+          const float4 Tc = trow[ctype >= 0 ? ctype : 0];
+          for (; j < hi; j += nthr) {
             const float4 pj = s_beads[j];
-            const float4 Tj = trow[bead_type(pj.w)];
-            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, true, A.K);
-            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, true, A.K);
+            const float4 Tj = ctype >= 0 ? Tc : trow[bead_type(pj.w)];
+            const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
+            const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pj, box, invbox), Tj.x, Tj.z);
             acc_o += en - eo;
           }
-          dcc += (double)acc_c;
-        } else {
-          for (int j = tid; j < N; j += nthr) {
-            if (j >= m0 && j < m0 + n) continue;
+        }
+      } else {
+        // a chain (or a multi-bead crowder): each thread takes its beads j and
+        // runs over the n moved beads k, the same k in every lane
+        const float4* oldp = same ? s_tpos + p_b * A.lmax : s_beads + m0;
+        const float4* newp = s_tpos + b * A.lmax;
+        for (int part = 0; part < 2; ++part) {
+          const int lo = part ? x1 : 0, hi = part ? N : x0;
+          if (lo >= hi) continue;
+          const int cb = min(hi, ncb);
+          int j = lo + ((tid - lo) & tmask);
+          for (; j < cb; j += nthr) {
             const float4 pj = s_beads[j];
             const int tb = bead_type(pj.w);
-            const float4 Tj = trow[tb];
-            const bool crowd = a_crowd || tb >= kNumAmino;
-            const float en = pair_energy_r2(pair_r2(pnew, pj, box, invbox), Tj, crowd, A.K);
-            const float eo = pair_energy_r2(pair_r2(pold, pj, box, invbox), Tj, crowd, A.K);
-            acc_o += en - eo;
+            float a = 0.0f;
+            if (!rec.crowd) {
+              for (int k = 0; k < n; ++k) {
+                const float4 po = oldp[k], pn = newp[k];
+                const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+                const float en = pair_energy_r2(pair_r2(pn, pj, box, invbox), T, false, A.K);
+                const float eo = pair_energy_r2(pair_r2(po, pj, box, invbox), T, false, A.K);
+                a += en - eo;
+              }
+              acc_c += a;
+            } else {
+              for (int k = 0; k < n; ++k) {
+                const float4 po = oldp[k], pn = newp[k];
+                const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+                const float en = crowd_energy<R12, CUT>(pair_r2(pn, pj, box, invbox), T.x, T.z);
+                const float eo = crowd_energy<R12, CUT>(pair_r2(po, pj, box, invbox), T.x, T.z);
+                a += en - eo;
+              }
+              acc_o += a;
+            }
+          }
+          for (; j < hi; j += nthr) {
+            const float4 pj = s_beads[j];
+            const int tb = bead_type(pj.w);
+            float a = 0.0f;
+            for (int k = 0; k < n; ++k) {
+              const float4 po = oldp[k], pn = newp[k];
+              const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+              const float en = crowd_energy<R12, CUT>(pair_r2(pn, pj, box, invbox), T.x, T.z);
+              const float eo = crowd_energy<R12, CUT>(pair_r2(po, pj, box, invbox), T.x, T.z);
+              a += en - eo;
+            }
+            acc_o += a;
           }
         }
-        dacc += (double)acc_o;
       }
-      // without crowders every pair of a chain move is a chain-chain pair
-      if (!rec.crowd && !split) dcc = dacc;
+      dcc = (double)acc_c;
+      dacc = (double)acc_o;
     }
     dacc = warp_sum(dacc);
-    if (split) dcc = warp_sum(dcc);
+    if (!rec.crowd) dcc = warp_sum(dcc);
     if (lane == 0) {
       s_red[b * 64 + warp] = dacc;
       s_red[b * 64 + 32 + warp] = dcc;
@@ -460,27 +517,32 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(SweepArgs A) {
     if ((s & 31) == 31) cp_async_wait_all();  // next ring half has landed
     __syncthreads();  // R: partial sums (and the prefetched records) visible
 
-    // ---- every thread: the same FP64 sums and the same Metropolis decision
-    double dE_cc = 0.0, dE = 0.0;
-    for (int w = 0; w < nwarps; ++w) dE += s_red[b * 64 + w];
-    if (split) {
-      for (int w = 0; w < nwarps; ++w) dE_cc += s_red[b * 64 + 32 + w];
+    // ---- every thread: the same FP64 sums (a fixed pairwise tree over the
+    // warps' partials) and the same Metropolis decision
+    if (s + 1 < n_steps && A.mol_in_smem == 0) {
+      // centre of the next step's molecule, loaded while this step finishes;
+      // if that molecule moves in this step, the next step takes the centre
+      // from registers instead (same && !p_rot)
+      next_c = cent[s_ring[(s + 1) & (kRing - 1)].m];
+    }
+    double dE = tree_sum8(s_red + b * 64, nwarps);
+    double dE_cc = 0.0;
+    if (!rec.crowd) {
+      dE_cc = tree_sum8(s_red + b * 64 + 32, nwarps);
       dE += dE_cc;
-    } else if (!rec.crowd) {
-      dE_cc = dE;  // no crowders: the whole change is chain-chain
     }
     const int acc = dE < 0.0 ? 1 : (dE < recs_.thr ? 2 : 0);
     if (acc) {
       energy += dE;
       ecc += dE_cc;
       if (n == 1) {
-        if (tid == m0 % nthr) s_beads[m0] = pnew1;
+        if (tid == (m0 & tmask)) s_beads[m0] = pnew1;
         p_single = pnew1;
       } else {
         // the owners install the chain (and its relative positions)
         QuatProducts qp{};
         if (rec.rotate) qp = quat_products(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3]);
-        int j = m0 + ((tid - m0 % nthr) + nthr) % nthr;
+        int j = m0 + ((tid - m0) & tmask);
         for (; j < m0 + n; j += nthr) {
           s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
           if (rec.rotate) {
@@ -611,11 +673,69 @@ struct TileItem {
 
 constexpr int kTile = 128;
 
+// Energy of bead i (position pi, type ta) against the j beads s_j[lo-j0 ..
+// hi-j0) of the tile, in ascending j, leaving out the beads [xa, xb) of its own
+// molecule. Beads are stored chains first, crowders after, so the range
+// splits into a chain part [lo, ncb) and a crowder part [ncb, hi), and each
+// part runs a loop specialised to its pair class:
+//   chain i, chain j ..... Kim-Hummer + Debye-Hueckel, table entry per pair
+//                          (added to the chain-chain sum as well);
+//   any i, crowder j ..... crowder wall with the table entry fixed per i when
+//                          the system has one crowder species;
+//   crowder i, chain j ... crowder wall, table entry per residue type.
+// The single accumulator runs in ascending j, as one unspecialised loop would.
+template <bool R12, bool CUT>
+__device__ __forceinline__ void energy_row(const float4* __restrict__ s_j, int j0, int lo, int hi,
+                                           int xa, int xb, int ncb, int ctype, float4 pi, int ta,
+                                           const float4* __restrict__ s_tab, float box,
+                                           float invbox, const EnergyConsts& K, float& acc,
+                                           float& acc_cc) {
+  const bool a_crowd = ta >= kNumAmino;
+  // two sub-ranges of [lo, hi) outside the own molecule
+  const int r0a = lo, r0b = min(hi, xa);
+  const int r1a = max(lo, xb), r1b = hi;
+  for (int part = 0; part < 2; ++part) {
+    const int a = part ? r1a : r0a, b = part ? r1b : r0b;
+    if (a >= b) continue;
+    const int cb = min(b, ncb);  // [a, cb): chain beads; [max(a, ncb), b): crowders
+    if (!a_crowd) {
+#pragma unroll 4
+      for (int j = a; j < cb; ++j) {
+        const float4 pj = s_j[j - j0];
+        const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
+        const float e = pair_energy_r2(pair_r2(pi, pj, box, invbox), T, false, K);
+        acc += e;
+        acc_cc += e;
+      }
+    } else {
+#pragma unroll 4
+      for (int j = a; j < cb; ++j) {
+        const float4 pj = s_j[j - j0];
+        const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
+        acc += crowd_energy<R12, CUT>(pair_r2(pi, pj, box, invbox), T.x, T.z);
+      }
+    }
+    const int ca = max(a, ncb);
+    if (ctype >= 0) {
+      const float4 T = s_tab[ctype * kNT + ta];
+#pragma unroll 4
+      for (int j = ca; j < b; ++j)
+        acc += crowd_energy<R12, CUT>(pair_r2(pi, s_j[j - j0], box, invbox), T.x, T.z);
+    } else {
+      for (int j = ca; j < b; ++j) {
+        const float4 pj = s_j[j - j0];
+        const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
+        acc += crowd_energy<R12, CUT>(pair_r2(pi, pj, box, invbox), T.x, T.z);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
-    const TileItem* __restrict__ items, int n_items, double* __restrict__ scratch,
-    double* __restrict__ scratch_cc, EnergyConsts K) {
+    const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
+    double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
   __shared__ double s_red[kTile / 32];
@@ -627,7 +747,6 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev S = sys[inst_sys[W.inst]];
     const int N = S.n_beads;
     const int base = S.bead_base + (W.inst - S.inst0) * N;
-    const float box = S.box, invbox = S.invbox;
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
     __syncthreads();  // previous item done with s_j
@@ -638,18 +757,23 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     if (i < N) {
       const float4 pi = pos[base + i];
       const int ta = bead_type(pi.w), mi = bead_mol(pi.w);
-      const bool a_crowd = ta >= kNumAmino;
-      const int jstart = (W.ti == W.tj) ? tid + 1 : 0;
+      const int xa = mol_start[S.mstart_off + mi], xb = mol_start[S.mstart_off + mi + 1];
+      const int lo = (W.ti == W.tj) ? i + 1 : j0;
       float acc = 0.0f, acc_cc = 0.0f;  // all pairs; chain-chain pairs
-      for (int jj = jstart; jj < jn; ++jj) {
-        const float4 pj = s_j[jj];
-        if (bead_mol(pj.w) == mi) continue;
-        const int tb = bead_type(pj.w);
-        const float4 Tij = s_tab[tb * kNT + ta];
-        const bool crowd = a_crowd || tb >= kNumAmino;
-        const float e = pair_energy_r2(pair_r2(pi, pj, box, invbox), Tij, crowd, K);
-        acc += e;
-        if (!crowd) acc_cc += e;
+      if (K.crowder_mode) {
+        if (K.crowder_cut)
+          energy_row<true, true>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
+                                 pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+        else
+          energy_row<true, false>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
+                                  pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+      } else {
+        if (K.crowder_cut)
+          energy_row<false, true>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
+                                  pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+        else
+          energy_row<false, false>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
+                                   pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
       }
       dsum = (double)acc;
       dcc = (double)acc_cc;
@@ -879,7 +1003,8 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
 }
 
 // Per-molecule force and torque about the centre (torque = sum rel x F):
-// one CTA per instance, one warp per molecule, FP64 sums.
+// one CTA per instance; one thread per one-bead molecule, one warp per chain
+// (FP64 sums).
 __global__ void molecule_force_torque_kernel(const SysDev* __restrict__ sys,
                                              const int* __restrict__ inst_sys,
                                              const int* __restrict__ mol_start,
@@ -892,8 +1017,26 @@ __global__ void molecule_force_torque_kernel(const SysDev* __restrict__ sys,
   const int base = S.bead_base + slot * S.n_beads;
   const int mbase = S.mol_base + slot * S.n_mol;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int* ms = mol_start + S.mstart_off;
+  // one-bead molecules (crowders): one thread each, no reduction
+  for (int m = threadIdx.x; m < S.n_mol; m += blockDim.x) {
+    const int a = ms[m];
+    if (ms[m + 1] - a != 1) continue;
+    const float4 rl = rel[base + a];
+    const double Fx = forces[3 * (size_t)(base + a)], Fy = forces[3 * (size_t)(base + a) + 1],
+                 Fz = forces[3 * (size_t)(base + a) + 2];
+    double* o = out + 6 * (size_t)(mbase + m);
+    o[0] = Fx;
+    o[1] = Fy;
+    o[2] = Fz;
+    o[3] = (double)rl.y * Fz - (double)rl.z * Fy;
+    o[4] = (double)rl.z * Fx - (double)rl.x * Fz;
+    o[5] = (double)rl.x * Fy - (double)rl.y * Fx;
+  }
+  // chains: one warp each
   for (int m = warp; m < S.n_mol; m += nw) {
-    const int a = mol_start[S.mstart_off + m], b = mol_start[S.mstart_off + m + 1];
+    const int a = ms[m], b = ms[m + 1];
+    if (b - a == 1) continue;
     double v[6] = {0, 0, 0, 0, 0, 0};
     for (int k = a + lane; k < b; k += 32) {
       const float4 rl = rel[base + k];
@@ -1171,6 +1314,7 @@ EnergyConsts consts_of(const remc_handle* h) {
   EnergyConsts K;
   K.c_xi = (float)(-1.4426950408889634 / (double)h->params.debye_length);
   K.crowder_mode = h->params.crowder_mode;
+  K.crowder_cut = h->params.crowder_cutoff > 0.0f ? 1 : 0;
   return K;
 }
 
@@ -1198,10 +1342,18 @@ int ensure_recs(remc_handle* h, size_t steps) {
   return REMC_OK;
 }
 
+// The sweep kernel compiled for the handle's crowder model.
+using SweepFn = void (*)(SweepArgs);
+SweepFn sweep_fn(const remc_params& p) {
+  const bool cut = p.crowder_cutoff > 0.0f;
+  if (p.crowder_mode) return cut ? sweep_kernel<true, true> : sweep_kernel<true, false>;
+  return cut ? sweep_kernel<false, true> : sweep_kernel<false, false>;
+}
+
 // Set the sweep schedule: threads per replica and where molecule data lives.
 int configure_sweep(remc_handle* h, int threads, int mol_in_smem) {
-  if (threads % 32 != 0 || threads < 32 || threads > 256)
-    return set_error(REMC_ERR_INVALID, "threads per replica must be a multiple of 32, <= 256");
+  if (threads < 32 || threads > 256 || (threads & (threads - 1)) != 0)
+    return set_error(REMC_ERR_INVALID, "threads per replica must be 32, 64, 128 or 256");
   const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem).total;
   if (smem > (size_t)h->max_dyn_smem)
     return set_error(REMC_ERR_INVALID,
@@ -1209,7 +1361,7 @@ int configure_sweep(remc_handle* h, int threads, int mol_in_smem) {
                      h->max_dyn_smem);
   int per_sm = 0;
   cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel, threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_fn(h->params), threads, smem);
   if (e != cudaSuccess || per_sm < 1)
     return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
                      cudaGetErrorString(e));
@@ -1303,7 +1455,7 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.lmax = h->lmax;
   A.K = consts_of(h);
   const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem).total;
-  sweep_kernel<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
+  sweep_fn(h->params)<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
   REMC_CUDA_TRY(cudaGetLastError());
   return REMC_OK;
 }
@@ -1408,7 +1560,19 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     S.invbox = 1.0f / d.box;
     S.translate_only_crowders = d.translate_only_crowders ? 1 : 0;
     S.n_chain_beads = 0;
-    for (int b = 0; b < d.n_beads; ++b) S.n_chain_beads += d.bead_type[b] < kNumAmino ? 1 : 0;
+    S.crowd_type = -1;
+    bool mixed = false;
+    for (int b = 0; b < d.n_beads; ++b) {
+      const int t = d.bead_type[b];
+      if (t < kNumAmino) {
+        ++S.n_chain_beads;
+      } else if (S.crowd_type < 0) {
+        S.crowd_type = t;
+      } else if (S.crowd_type != t) {
+        mixed = true;
+      }
+    }
+    if (mixed) S.crowd_type = -1;
     h->h_sys.push_back(S);
     for (int k = 0; k < d.n_replicas; ++k) h->h_inst_sys.push_back(s);
     h->h_mol_start.insert(h->h_mol_start.end(), d.mol_start, d.mol_start + d.n_mol + 1);
@@ -1439,18 +1603,26 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   int max_smem = 0;
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  cudaFuncAttributes fattr;
-  e = cudaFuncGetAttributes(&fattr, sweep_kernel);
-  if (e != cudaSuccess) {
-    delete h;
-    return set_error(REMC_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+  const SweepFn kSweeps[4] = {sweep_kernel<false, false>, sweep_kernel<false, true>,
+                              sweep_kernel<true, false>, sweep_kernel<true, true>};
+  int static_smem = 0;
+  for (SweepFn f : kSweeps) {
+    cudaFuncAttributes fattr;
+    e = cudaFuncGetAttributes(&fattr, f);
+    if (e != cudaSuccess) {
+      delete h;
+      return set_error(REMC_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+    }
+    static_smem = std::max(static_smem, (int)fattr.sharedSizeBytes);
   }
-  const int max_dyn = max_smem - (int)fattr.sharedSizeBytes;
+  const int max_dyn = max_smem - static_smem;
   h->max_dyn_smem = max_dyn;
-  e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn);
-  if (e != cudaSuccess) {
-    delete h;
-    return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+  for (SweepFn f : kSweeps) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn);
+    if (e != cudaSuccess) {
+      delete h;
+      return set_error(REMC_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
   }
   // default schedule (the autotuner may replace it): molecule data in shared
   // memory when it fits, more threads per replica for larger systems
@@ -1590,6 +1762,7 @@ int remc_set_params(remc_handle* h, const remc_params* p) {
   if (!(p->debye_length > 0.0f) || (p->crowder_mode != 0 && p->crowder_mode != 1))
     return set_error(REMC_ERR_INVALID, "bad parameters");
   h->params = *p;
+  h->config_gen++;  // a captured graph holds the old constants and kernel
   if (h->tables_set) return build_tables(h);
   return REMC_OK;
 }
@@ -1728,8 +1901,8 @@ int remc_energy_full(remc_handle* h, double* out) {
   if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   int grid = std::min(h->n_items, h->num_sms * 8);
   energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
-                                                   h->d_items, h->n_items, h->d_scratch,
-                                                   h->d_scratch_cc, consts_of(h));
+                                                   h->d_mol_start, h->d_items, h->n_items,
+                                                   h->d_scratch, h->d_scratch_cc, consts_of(h));
   REMC_CUDA_TRY(cudaGetLastError());
   energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(
       h->d_item_off, h->n_inst, h->d_scratch, h->d_scratch_cc, h->d_energy, h->d_ecc);

@@ -283,7 +283,7 @@ def test_autotune_restores_state_and_schedules_agree(built_lib):
     s = w.systems[0]
     R = 4
     outs = []
-    for sched in ("tuned", (128, True), (256, False)):
+    for sched in ("tuned", (128, True), (256, False), (64, True)):
         with _engine([s], R, w.params) as eng:
             eng.set_replica_params([w.ladders[0][:R]], np.full(R, 0.5, np.float32),
                                    np.full(R, 0.2))
@@ -299,6 +299,9 @@ def test_autotune_restores_state_and_schedules_agree(built_lib):
                 assert np.array_equal(e_before, eng.energies())
                 assert all(c.sum() == 0 for c in eng.counters())
             else:
+                eng.set_schedule(*sched)
+                with pytest.raises(Exception):
+                    eng.set_schedule(96, True)  # thread counts are powers of two
                 eng.set_schedule(*sched)
             eng.sweep(400, 11, 0)
             outs.append((eng.download_state(), eng.energies()))
