@@ -833,12 +833,107 @@ struct AdjConsts {
   float inv_xi2;  // 1/Xi^2
 };
 
+// Forces of one j group of 8 on this lane's bead i, and the group's j forces
+// summed over the warp into s_fj. Lane L takes the 8 beads in the order
+// j = jg + (q ^ r), r = (L >> 2) & 7, so that every level of the
+// recursive-halving transpose-reduce keeps and sends fixed registers:
+// after the xor-16, xor-8 and xor-4 levels and the xor-2/xor-1 sums, the four
+// lanes of group r hold the warp's total force from bead jg + r.
+// CHAIN: beads [jg, jend) are residues (Kim-Hummer + Debye-Hueckel against a
+// residue i, crowder wall against a crowder i); else crowders (wall).
+// CHECK = false when every lane's 8 pairs are known to count.
+template <bool R12, bool CUT, bool CHAIN, bool CHECK>
+__device__ __forceinline__ void adjoint_group(
+    const float4* __restrict__ s_j, const float4* __restrict__ s_tab, float* __restrict__ s_G,
+    float (*__restrict__ s_fjw)[3], int jg, int jend, int jlo, int ex0, int ex1, bool ivalid,
+    float4 pi, int ta, bool a_crowd, float4 Tc, bool tc_fixed, float box, float invbox,
+    const EnergyConsts& K, const AdjConsts& C, int lane, float& fx, float& fy, float& fz,
+    float& acc_e, float& acc_x) {
+  const int r = (lane >> 2) & 7;
+  float g[8][3];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    g[q][0] = g[q][1] = g[q][2] = 0.0f;
+    const int jj = jg + (q ^ r);
+    if (CHECK) {
+      const bool valid = ivalid && jj < jend && jj >= jlo &&
+                         (unsigned)(jj - ex0) >= (unsigned)(ex1 - ex0);
+      if (!valid) continue;
+    }
+    const float4 pj = s_j[jj];
+    const float dx = min_image(pi.x - pj.x, box, invbox);
+    const float dy = min_image(pi.y - pj.y, box, invbox);
+    const float dz = min_image(pi.z - pj.z, box, invbox);
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float rinv = fast_rsqrt(r2);
+    const float rinv2 = rinv * rinv;
+    float f;  // -(de/dr)/r
+    if (CHAIN && !a_crowd) {
+      const int tb = bead_type(pj.w);
+      const float4 T = s_tab[tb * kNT + ta];
+      const float s2 = T.y * rinv2;
+      const float s6 = s2 * s2 * s2;
+      const float gg = fmaf(-s6, s6, s6);  // s6 (1 - s6)
+      float lj = T.x * gg;
+      float dlj = 6.0f * T.x * s6 * fmaf(-2.0f, s6, 1.0f) * rinv2;  // -(dLJ/dr)/r
+      float dg = 4.0f * gg;                                          // d e_LJ / d eps per c_lj
+      if (r2 < T.z) {
+        lj = fmaf(0.5f, T.x, -lj);
+        dlj = -dlj;
+        dg = 2.0f - dg;
+      }
+      const float rr = r2 * rinv;
+      const float dh = T.w * fast_ex2(rr * K.c_xi) * rinv;
+      acc_e += lj + dh;
+      acc_x += dh * rr;  // * 1/Xi^2 by the caller
+      f = dlj + dh * (C.inv_xi + rinv) * rinv;
+      atomicAdd(&s_G[ta * kNumAmino + tb], dg * C.c_lj);
+    } else {
+      const float4 T = (!CHAIN && tc_fixed) ? Tc : s_tab[bead_type(pj.w) * kNT + ta];
+      const float e = crowd_energy<R12, CUT>(r2, T.x, T.z);
+      acc_e += e;
+      f = (R12 ? 12.0f : 6.0f) * e * rinv2;
+    }
+    const float gx = f * dx, gy = f * dy, gz = f * dz;
+    fx += gx;
+    fy += gy;
+    fz += gz;
+    g[q][0] = gx;
+    g[q][1] = gy;
+    g[q][2] = gz;
+  }
+  float h4[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h4[q][c] = g[q][c] + __shfl_xor_sync(0xffffffffu, g[q + 4][c], 16);
+  float h2[2][3];
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h2[q][c] = h4[q][c] + __shfl_xor_sync(0xffffffffu, h4[q + 2][c], 8);
+  float h1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h1[c] = h2[0][c] + __shfl_xor_sync(0xffffffffu, h2[1][c], 4);
+    h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 2);
+    h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 1);
+  }
+  if ((lane & 3) == 0 && jg + r < jend) {
+    // force on j = -(sum of the forces this warp's i beads feel from j)
+    s_fjw[jg + r][0] -= h1[0];
+    s_fjw[jg + r][1] -= h1[1];
+    s_fjw[jg + r][2] -= h1[2];
+  }
+}
+
+template <bool R12, bool CUT>
 __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
-    const TileItem* __restrict__ items, int n_items, float* __restrict__ forces,
-    double* __restrict__ G, double* __restrict__ dxi, double* __restrict__ e_out,
-    EnergyConsts K, AdjConsts C) {
+    const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
+    float* __restrict__ forces, double* __restrict__ G, double* __restrict__ dxi,
+    double* __restrict__ e_out, EnergyConsts K, AdjConsts C) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
   __shared__ float s_fj[kTile / 32][kTile][3];
@@ -862,110 +957,37 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     const int i = W.ti * kTile + tid;
     const bool ivalid = i < N;
     float4 pi = ivalid ? pos[base + i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const int ta = bead_type(pi.w), mi = ivalid ? bead_mol(pi.w) : -1;
+    const int ta = bead_type(pi.w);
     const bool a_crowd = ta >= kNumAmino;
-    float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
-    // j beads in groups of 8: each lane computes its pair with all 8, then a
-    // recursive-halving transpose-reduce sums the 8 j forces over the warp
-    // (27 shuffles for 8 x 3 components instead of 120 for per-j trees)
-    for (int jg = 0; jg < jn; jg += 8) {  // uniform trip count
-      float g[8][3];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        g[q][0] = g[q][1] = g[q][2] = 0.0f;
-        const int jj = jg + q;
-        if (jj >= jn) continue;
-        const float4 pj = s_j[jj];
-        const int tb = bead_type(pj.w);
-        const bool valid = ivalid && (W.ti != W.tj || jj > tid) && bead_mol(pj.w) != mi;
-        if (!valid) continue;
-        const float dx = min_image(pi.x - pj.x, box, invbox);
-        const float dy = min_image(pi.y - pj.y, box, invbox);
-        const float dz = min_image(pi.z - pj.z, box, invbox);
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float rinv = fast_rsqrt(r2);
-        const float rinv2 = rinv * rinv;
-        const float4 T = s_tab[tb * kNT + ta];
-        float f;  // -(de/dr)/r
-        if (a_crowd || tb >= kNumAmino) {
-          const float i6 = rinv2 * rinv2 * rinv2;
-          float e = T.x * i6;
-          float pw = 6.0f;
-          if (K.crowder_mode) {
-            e *= i6;
-            pw = 12.0f;
-          }
-          if (!(r2 < T.z)) e = 0.0f;
-          acc_e += e;
-          f = pw * e * rinv2;
-        } else {
-          const float s2 = T.y * rinv2;
-          const float s6 = s2 * s2 * s2;
-          const float gg = fmaf(-s6, s6, s6);           // s6 (1 - s6)
-          float lj = T.x * gg;
-          float dlj = 6.0f * T.x * s6 * fmaf(-2.0f, s6, 1.0f) * rinv2;  // -(dLJ/dr)/r
-          float dg = 4.0f * gg;                         // d e_LJ / d eps per c_lj
-          if (r2 < T.z) {
-            lj = fmaf(0.5f, T.x, -lj);
-            dlj = -dlj;
-            dg = 2.0f - dg;
-          }
-          const float r = r2 * rinv;
-          const float dh = T.w * fast_ex2(r * K.c_xi) * rinv;
-          acc_e += lj + dh;
-          acc_x += dh * r;                              // * 1/Xi^2 below
-          f = dlj + dh * (C.inv_xi + rinv) * rinv;
-          if (ta < kNumAmino && tb < kNumAmino) atomicAdd(&s_G[ta * kNumAmino + tb], dg * C.c_lj);
-        }
-        const float gx = f * dx, gy = f * dy, gz = f * dz;
-        fx += gx;
-        fy += gy;
-        fz += gz;
-        g[q][0] = gx;
-        g[q][1] = gy;
-        g[q][2] = gz;
-      }
-      // level 1 (lane bit 4): keep j 0-3 or 4-7
-      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-      float h4[4][3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float keep = b4 ? g[q + 4][c] : g[q][c];
-          const float send = b4 ? g[q][c] : g[q + 4][c];
-          h4[q][c] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-        }
-      // level 2 (bit 3): keep 2 of the 4
-      float h2[2][3];
-#pragma unroll
-      for (int q = 0; q < 2; ++q)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float keep = b3 ? h4[q + 2][c] : h4[q][c];
-          const float send = b3 ? h4[q][c] : h4[q + 2][c];
-          h2[q][c] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-        }
-      // level 3 (bit 2): keep 1, then sum the remaining two lane bits
-      float h1[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float keep = b2 ? h2[1][c] : h2[0][c];
-        const float send = b2 ? h2[0][c] : h2[1][c];
-        h1[c] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-        h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 2);
-        h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 1);
-      }
-      if ((lane & 3) == 0) {
-        const int q = (b4 ? 4 : 0) + (b3 ? 2 : 0) + (b2 ? 1 : 0);
-        if (jg + q < jn) {
-          // force on j = -(sum of the forces this warp's i beads feel from j)
-          s_fj[warp][jg + q][0] -= h1[0];
-          s_fj[warp][jg + q][1] -= h1[1];
-          s_fj[warp][jg + q][2] -= h1[2];
-        }
-      }
+    // j (relative to j0) runs from jlo, leaving out the own molecule [ex0, ex1)
+    const int jlo = (W.ti == W.tj) ? tid + 1 : 0;
+    int ex0 = 0, ex1 = 0;
+    if (ivalid) {
+      const int mi = bead_mol(pi.w);
+      ex0 = mol_start[S.mstart_off + mi] - j0;
+      ex1 = mol_start[S.mstart_off + mi + 1] - j0;
     }
+    const int jc = max(0, min(jn, S.n_chain_beads - j0));  // [0, jc) residues, [jc, jn) crowders
+    const bool tc_fixed = S.crowd_type >= 0;
+    const float4 Tc = s_tab[(tc_fixed ? S.crowd_type : 0) * kNT + ta];
+    float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
+    // a group needs no per-pair tests when, for every lane, it is full, past
+    // the lane's first j and clear of its own molecule (a warp vote)
+#define REMC_ADJ_GROUP(CHAIN_, jend_)                                                           \
+  {                                                                                          \
+    const bool clean = ivalid && jg + 8 <= (jend_) && jg >= jlo && (ex1 <= jg || ex0 >= jg + 8); \
+    if (__all_sync(0xffffffffu, clean))                                                      \
+      adjoint_group<R12, CUT, CHAIN_, false>(s_j, s_tab, s_G, s_fj[warp], jg, jend_, jlo, ex0, \
+                                             ex1, ivalid, pi, ta, a_crowd, Tc, tc_fixed, box, \
+                                             invbox, K, C, lane, fx, fy, fz, acc_e, acc_x);   \
+    else                                                                                     \
+      adjoint_group<R12, CUT, CHAIN_, true>(s_j, s_tab, s_G, s_fj[warp], jg, jend_, jlo, ex0, \
+                                            ex1, ivalid, pi, ta, a_crowd, Tc, tc_fixed, box,  \
+                                            invbox, K, C, lane, fx, fy, fz, acc_e, acc_x);    \
+  }
+    for (int jg = 0; jg < jc; jg += 8) REMC_ADJ_GROUP(true, jc)  // uniform trip counts
+    for (int jg = jc; jg < jn; jg += 8) REMC_ADJ_GROUP(false, jn)
+#undef REMC_ADJ_GROUP
     double de = warp_sum((double)acc_e), dxv = warp_sum((double)acc_x);
     if (lane == 0) {
       s_red[warp][0] = de;
@@ -2159,9 +2181,14 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
   C.inv_xi2 = C.inv_xi * C.inv_xi;
   C.c_lj = (float)((double)h->params.lj_cf * (double)h->params.kbt_cf);
   const int grid = std::min(h->n_items, h->num_sms * 8);
-  adjoint_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
-                                                    h->d_items, h->n_items, h->d_forces, h->d_G,
-                                                    h->d_dxi, h->d_eadj, consts_of(h), C);
+  const bool cut = h->params.crowder_cutoff > 0.0f;
+  auto adj = h->params.crowder_mode ? (cut ? adjoint_tile_kernel<true, true>
+                                           : adjoint_tile_kernel<true, false>)
+                                    : (cut ? adjoint_tile_kernel<false, true>
+                                           : adjoint_tile_kernel<false, false>);
+  adj<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab, h->d_mol_start,
+                                     h->d_items, h->n_items, h->d_forces, h->d_G, h->d_dxi,
+                                     h->d_eadj, consts_of(h), C);
   REMC_CUDA_TRY(cudaGetLastError());
   molecule_force_torque_kernel<<<h->n_inst, 256, 0, h->stream>>>(
       h->d_sys, h->d_inst_sys, h->d_mol_start, h->d_rel, h->d_forces, h->d_mft);
