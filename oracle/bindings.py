@@ -243,6 +243,10 @@ def ref_lib():
         L.ref_random_vectors.argtypes = [C.c_void_p, PD, PF, PD]
         L.ref_time_mcsearch.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int]
         L.ref_time_mcsearch.restype = C.c_double
+        L.ref_run_mcsearch.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int]
+        L.ref_run_mcsearch.restype = C.c_double
+        L.ref_replica_seed.argtypes = [C.c_void_p, C.c_uint]
+        L.ref_replica_counters.argtypes = [C.c_void_p, PI]
         _rlib = L
     return _rlib
 
@@ -317,6 +321,15 @@ class ReferenceReplica:
     def steps_set(self, translate_step: float, rotate_step: float) -> None:
         self.set_steps(translate_step, rotate_step)
 
+    def seed(self, seed: int) -> None:
+        """Leave fed mode; seed the replica's own MT19937 generators."""
+        ref_lib().ref_replica_seed(self.h, seed)
+
+    def counters(self):
+        out = np.zeros(3, np.int32)
+        ref_lib().ref_replica_counters(self.h, _p(out, C.c_int))
+        return tuple(int(x) for x in out)
+
     def mcsearch(self, u: np.ndarray):
         """Run len(u) reference MCSearch steps fed with u[s] = 6 uniforms."""
         u = np.ascontiguousarray(u, np.float64).reshape(-1, 6)
@@ -327,6 +340,14 @@ class ReferenceReplica:
         under = ref_lib().ref_replica_mcsearch(self.h, n, _p(u, C.c_double), _p(flags, C.c_int),
                                                _p(mol, C.c_int), _p(en, C.c_double))
         return flags, mol, en, under
+
+
+def run_reference_mcsearch(replicas, n_threads: int, n_steps: int) -> float:
+    """The reference's own MCSearch(n_steps) with its own generators (seed
+    them first with ReferenceReplica.seed) on every replica, spread over
+    n_threads host threads; returns wall seconds."""
+    arr = (C.c_void_p * len(replicas))(*[r.h for r in replicas])
+    return ref_lib().ref_run_mcsearch(arr, len(replicas), n_threads, n_steps)
 
 
 def time_reference_mcsearch(replicas, n_threads: int, n_steps: int) -> float:

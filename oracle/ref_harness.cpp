@@ -248,26 +248,39 @@ void ref_random_vectors(void* hp, const double* u3, float* vf, double* vd) {
   vd[0] = b.x; vd[1] = b.y; vd[2] = b.z;
 }
 
-// Timing driver for the CPU baseline: the reference's own Replica::MCSearch
-// (Replica.cpp:368-478, full Replica::E() every step, MT19937 draws) on
-// `n` replicas spread over `n_threads` host threads, replicas assigned to
-// threads in contiguous slices as MCthreadableFunction does
-// (main.cpp:879-883). The replicas must not be in fed mode. Returns wall
-// seconds. (The reference executable itself cannot load more than 30
+// Timing driver for the CPU baseline (ref_time_mcsearch below): the
+// reference's own Replica::MCSearch (Replica.cpp:368-478, full Replica::E()
+// every step, MT19937 draws) on replicas spread over host threads, after
+// seeding each. (The reference executable itself cannot load more than 30
 // molecules: Replica::loadMolecule grows its array with a shallow memcpy and
 // the deleted originals free the file names the copies still hold.)
-double ref_time_mcsearch(void** handles, int n, int n_threads, int n_steps) {
+// Leave fed mode and seed the replica's seven MT19937 generators (from
+// `seed`), as Replica::initRNGs does from the clock (Replica.cpp:265-300).
+void ref_replica_seed(void* hp, unsigned seed) {
+  Replica& r = ((Harness*)hp)->rep;
+  gsl_rng* all[7] = {r.rng_moleculeSelection, r.MCRng, r.rng_rotate, r.rng_translate,
+                     r.MCKbRng, r.rng_rotateAmount, r.rng_translateAmount};
+  for (int k = 0; k < 7; ++k) {
+    all[k]->fed = 0;
+    gsl_rng_set(all[k], 7u * seed + (unsigned)k + 1u);
+  }
+}
+
+// accept, acceptA, reject of the replica (Replica.h:120-122).
+void ref_replica_counters(void* hp, int* out) {
+  Replica& r = ((Harness*)hp)->rep;
+  out[0] = r.accept;
+  out[1] = r.acceptA;
+  out[2] = r.reject;
+}
+
+// The reference's own Replica::MCSearch(n_steps) on `n` replicas over
+// `n_threads` host threads, replicas assigned in contiguous slices as
+// MCthreadableFunction does (main.cpp:879-883), with their own generators
+// (not fed). Returns wall seconds.
+double ref_run_mcsearch(void** handles, int n, int n_threads, int n_steps) {
   if (n_threads < 1) n_threads = 1;
   if (n_threads > n) n_threads = n;
-  for (int i = 0; i < n; ++i) {
-    Replica& r = ((Harness*)handles[i])->rep;
-    gsl_rng* all[7] = {r.rng_moleculeSelection, r.MCRng, r.rng_rotate, r.rng_translate,
-                       r.MCKbRng, r.rng_rotateAmount, r.rng_translateAmount};
-    for (int k = 0; k < 7; ++k) {
-      all[k]->fed = 0;
-      gsl_rng_set(all[k], 1000u + 7u * (unsigned)i + (unsigned)k);
-    }
-  }
   auto t0 = std::chrono::steady_clock::now();
   std::vector<std::thread> pool;
   const int per = (n + n_threads - 1) / n_threads;
@@ -279,6 +292,11 @@ double ref_time_mcsearch(void** handles, int n, int n_threads, int n_steps) {
   }
   for (auto& th : pool) th.join();
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+double ref_time_mcsearch(void** handles, int n, int n_threads, int n_steps) {
+  for (int i = 0; i < n; ++i) ref_replica_seed(handles[i], 1000u + (unsigned)i);
+  return ref_run_mcsearch(handles, n, n_threads, n_steps);
 }
 
 }  // extern "C"
