@@ -78,6 +78,10 @@ def oracle_lib():
         L.oracle_exchange_round.argtypes = [C.c_int, C.c_int, PF, PD, PI, PI, C.c_uint64,
                                             C.c_uint32, C.c_uint32, PI]
         L.oracle_exchange_round.restype = C.c_int
+        L.oracle_post_rebuild.argtypes = [PF, PI, C.c_int, PI, PF, C.c_float, PD, PF, PF]
+        L.oracle_post_drms.argtypes = [PF, PF, PI, C.c_int, C.c_int, C.c_float, C.c_float,
+                                       C.POINTER(C.c_longlong)]
+        L.oracle_post_drms.restype = C.c_double
         L.oracle_energy_adjoint.argtypes = [C.POINTER(OracleSystem), C.POINTER(OracleParams),
                                             PF, PF, PD, PD, PD, PD]
         _olib = L
@@ -100,6 +104,33 @@ def step_uniforms(seed: int, step: int, slot: int, system: int) -> np.ndarray:
 
 def exchange_uniform(seed: int, round_: int, pair: int, system: int) -> float:
     return oracle_lib().oracle_exchange_uniform(seed, round_, pair, system)
+
+
+def post_rebuild(rel0, mol_start, shift, centre0, box, quat, centre):
+    """pdbgen's pose reconstruction of one frame (oracle_post_rebuild)."""
+    rel0 = np.ascontiguousarray(rel0, np.float32)
+    ms = np.ascontiguousarray(mol_start, np.int32)
+    sh = np.ascontiguousarray(shift, np.int32)
+    c0 = np.ascontiguousarray(centre0, np.float32)
+    q = np.ascontiguousarray(quat, np.float64)
+    c = np.ascontiguousarray(centre, np.float32)
+    pos = np.zeros((int(ms[-1]), 3), np.float32)
+    oracle_lib().oracle_post_rebuild(_p(rel0, C.c_float), _p(ms, C.c_int), len(ms) - 1,
+                                     _p(sh, C.c_int), _p(c0, C.c_float), box, _p(q, C.c_double),
+                                     _p(c, C.c_float), _p(pos, C.c_float))
+    return pos
+
+
+def post_drms(sim, ref, mol_start, reverse=False, native_cut=12.0, recovered_cut=15.0):
+    """DRMS of one frame and its (native, recovered, binding) contact counts."""
+    x = np.ascontiguousarray(sim, np.float32)
+    r = np.ascontiguousarray(ref, np.float32)
+    ms = np.ascontiguousarray(mol_start, np.int32)
+    cnt = np.zeros(3, np.int64)
+    d = oracle_lib().oracle_post_drms(_p(x, C.c_float), _p(r, C.c_float), _p(ms, C.c_int),
+                                      len(ms) - 1, 1 if reverse else 0, native_cut, recovered_cut,
+                                      cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
+    return d, cnt
 
 
 def params_from(p) -> OracleParams:

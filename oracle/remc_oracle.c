@@ -439,3 +439,106 @@ void oracle_energy_adjoint(const oracle_system* s, const oracle_params* p, const
   *dE_dlambda = dl;
   *dE_dxi = dx;
 }
+
+/* ----------------------------------------------------------- post-processing */
+static void post_normalize(double q[4]) {
+  double m = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  q[0] /= m;
+  q[1] /= m;
+  q[2] /= m;
+  q[3] /= m;
+}
+
+/* Quaternion::rotateVector (Quaternion.cpp:84-101), FP64, result rounded to FP32. */
+static void post_rotate(const double q[4], const float* v, float* out) {
+  double w = q[0], x = q[1], y = q[2], z = q[3];
+  double w2 = w * w, x2 = x * x, y2 = y * y, z2 = z * z;
+  double wx = w * x, wy = w * y, wz = w * z, xy = x * y, xz = x * z, yz = y * z;
+  double vx = v[0], vy = v[1], vz = v[2];
+  out[0] = (float)(vx * (w2 + x2 - y2 - z2) + (vy * (xy - wz) + vz * (wy + xz)) * 2.0);
+  out[1] = (float)((vx * (wz + xy) + vz * (yz - wx)) * 2.0 + vy * (w2 - x2 + y2 - z2));
+  out[2] = (float)((vx * (xz - wy) + vy * (yz + wx)) * 2.0 + vz * (w2 - x2 - y2 + z2));
+}
+
+/* positioni -= boundary * round(v / boundary), v = positioni - molecule 0's
+ * position, per axis in FP32 (pdbgen.cpp:196-203) */
+static void post_image(float* c, const float* p, float box) {
+  for (int k = 0; k < 3; ++k) {
+    float v = c[k] - p[k];
+    c[k] -= box * roundf(v / box);
+  }
+}
+
+void oracle_post_rebuild(const float* rel0, const int* mol_start, int n_mol, const int* shift,
+                         const float* centre0, float box, const double* quat,
+                         const float* centre, float* pos) {
+  float p0[3] = {centre[0], centre[1], centre[2]};
+  if (shift[0]) post_image(p0, centre0, box);
+  for (int m = 0; m < n_mol; ++m) {
+    double q[4] = {quat[4 * m], quat[4 * m + 1], quat[4 * m + 2], quat[4 * m + 3]};
+    post_normalize(q); /* pdbgen.cpp:191 */
+    post_normalize(q); /* Molecule::setRotation (Molecule.cpp:335-346) */
+    float c[3] = {centre[3 * m], centre[3 * m + 1], centre[3 * m + 2]};
+    if (m == 0) {
+      c[0] = p0[0];
+      c[1] = p0[1];
+      c[2] = p0[2];
+    } else if (shift[m]) {
+      post_image(c, p0, box);
+    }
+    for (int b = mol_start[m]; b < mol_start[m + 1]; ++b) {
+      float r[3];
+      post_rotate(q, rel0 + 3 * b, r);
+      pos[3 * b] = r[0] + c[0];
+      pos[3 * b + 1] = r[1] + c[1];
+      pos[3 * b + 2] = r[2] + c[2];
+    }
+  }
+}
+
+/* Vector3f::magnitude of a - b (post processor/pdbgensrc/vector3f.h:35). */
+static float post_dist(const float* a, const float* b) {
+  float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return sqrtf(dx * dx + dy * dy + dz * dz);
+}
+
+double oracle_post_drms(const float* sim, const float* ref, const int* mol_start, int n_mol,
+                        int reverse, float native_cut, float recovered_cut, long long* counts) {
+  double drms = 0.0, N = 0.0;
+  long long nat = 0, rec = 0, bind = 0;
+  for (int I = 0; I < n_mol; ++I)
+    for (int J = I + 1; J < n_mol; ++J)
+      for (int i = mol_start[I]; i < mol_start[I + 1]; ++i)
+        for (int j = mol_start[J]; j < mol_start[J + 1]; ++j) {
+          N += 1.0;
+          float ds = post_dist(sim + 3 * i, sim + 3 * j);
+          float de = post_dist(ref + 3 * i, ref + 3 * j);
+          drms += fabsf(ds - de);
+          if (de < native_cut) {
+            ++nat;
+            if (ds < recovered_cut) ++rec;
+          }
+          if (ds < native_cut) ++bind;
+        }
+  drms /= N;
+  if (reverse) {
+    double drms2 = 0.0;
+    for (int I = 0; I < n_mol; ++I)
+      for (int J = I + 1; J < n_mol; ++J)
+        for (int i = mol_start[I]; i < mol_start[I + 1]; ++i)
+          for (int j = mol_start[J]; j < mol_start[J + 1]; ++j) {
+            int li = i - mol_start[I], lj = j - mol_start[J];
+            float ds = post_dist(sim + 3 * i, sim + 3 * j);
+            float dr = post_dist(ref + 3 * (mol_start[J] + li), ref + 3 * (mol_start[I] + lj));
+            drms2 += fabsf(ds - dr);
+          }
+    drms2 /= N;
+    if (drms2 < drms) drms = drms2;
+  }
+  if (counts) {
+    counts[0] = nat;
+    counts[1] = rec;
+    counts[2] = bind;
+  }
+  return drms;
+}

@@ -135,6 +135,22 @@ void oracle_energy_adjoint(const oracle_system* s, const oracle_params* p, const
                            const float* raw_table, double* forces, double* dE_dlambda,
                            double* dE_dxi, double* dE_deps);
 
+/* Post-processing.
+ * oracle_post_rebuild: pdbgen's pose reconstruction
+ * (post processor/pdbgensrc/pdbgen.cpp:166-215): quaternion normalised twice
+ * (pdbgen, Molecule::setRotation, Quaternion.cpp:18-27), rel0 rotated by
+ * Quaternion::rotateVector, shifted centres moved to the image nearest
+ * molecule 0 (molecule 0 against centre0), bead = rel + centre (FP32).
+ * oracle_post_drms: DRMS(Replica*, Replica*, bool)
+ * (post processor/pdbgensrc/drms.cpp:7-57) in its loop order, and the contact
+ * counts of DRMS(Replica*, Replica*) (simulation engine/src/main.cpp:789-836)
+ * with the thresholds as arguments. One frame per call. */
+void oracle_post_rebuild(const float* rel0, const int* mol_start, int n_mol, const int* shift,
+                         const float* centre0, float box, const double* quat,
+                         const float* centre, float* pos);
+double oracle_post_drms(const float* sim, const float* ref, const int* mol_start, int n_mol,
+                        int reverse, float native_cut, float recovered_cut, long long* counts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import re
 import os
 from typing import Iterable, List, Optional, Sequence
 
@@ -224,6 +225,7 @@ class Molecule:
     quat: np.ndarray       # float64[4]
     crowder: bool = False
     name: str = ""
+    res_seq: Optional[np.ndarray] = None  # PDB residue numbers (Residue::resSeq)
 
     @property
     def n(self) -> int:
@@ -249,12 +251,15 @@ class Molecule:
 
     @staticmethod
     def from_pdb(path: str, table: AminoAcidTable) -> "Molecule":
-        types, xyz = read_pdb_ca(path, table)
-        return Molecule.from_beads(types, xyz, name=path)
+        types, xyz, seq = read_pdb_ca(path, table, with_seq=True)
+        m = Molecule.from_beads(types, xyz, name=path)
+        m.res_seq = seq
+        return m
 
     def copy(self) -> "Molecule":
         return Molecule(self.types.copy(), self.pos.copy(), self.rel.copy(), self.centre.copy(),
-                        self.quat.copy(), self.crowder, self.name)
+                        self.quat.copy(), self.crowder, self.name,
+                        None if self.res_seq is None else self.res_seq.copy())
 
     def translate(self, v) -> None:
         """Molecule::translate: centre and every bead += v (FP32)."""
@@ -312,7 +317,7 @@ def normalise_axis(rx: float, ry: float, rz: float):
 
 
 # ------------------------------------------------------------------ PDB
-def read_pdb_ca(path: str, table: AminoAcidTable):
+def read_pdb_ca(path: str, table: AminoAcidTable, with_seq: bool = False):
     """CA beads of a PDB file, as Molecule::initFromPDB reads them.
 
     Fixed columns: atom name 13-16, residue name 18-20, x/y/z 31-38/39-46/47-54.
@@ -329,6 +334,7 @@ def read_pdb_ca(path: str, table: AminoAcidTable):
     # and that empty read is processed once more before eof stops the loop
     types: List[int] = []
     xyz: List[List[float]] = []
+    seq: List[int] = []
     prev = ""
     for ln in raw:
         ln = ln.rstrip("\r")[:511]
@@ -350,8 +356,12 @@ def read_pdb_ca(path: str, table: AminoAcidTable):
         z = _scanf_float(cur[46:54])
         types.append(t)
         xyz.append([x, y, z])
+        m = re.match(r"\s*[-+]?\d+", cur[22:26])  # resSeq, columns 23-26 (sscanf %d)
+        seq.append(int(m.group(0)) if m else 0)
     if not types:
         raise ModelError("%s: no CA atoms" % path)
+    if with_seq:
+        return np.array(types, np.int32), np.array(xyz, np.float32), np.array(seq, np.int32)
     return np.array(types, np.int32), np.array(xyz, np.float32)
 
 
