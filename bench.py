@@ -389,6 +389,7 @@ def main():
                        "l2": "256 MB buffer written between timed steps, outside the timing",
                        "schedule": {"threads_per_replica": sched_threads,
                                     "molecule_data_in_shared_memory": sched_smem,
+                                    "ctas_per_replica": eng.schedule()[2],
                                     "chosen_by": "remc_autotune"},
                        "parallelism": "replicas" if world == 1 else "weak: %d independent batches" % world},
             "pair_energies_per_s": pair_evals_all / t_max,

@@ -208,15 +208,22 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
              uint32_t round0);
 
 /* Autotuner: times a probe sweep of probe_steps steps for each candidate
- * schedule (threads per replica 128 or 256; molecule centres and starts in
- * shared or global memory) on the handle's own systems, restores the state
- * after every probe, and keeps the fastest. Outputs (may be NULL): the chosen
+ * schedule (threads per replica 128 or 256; molecule centres in shared or
+ * global memory; CTAs per replica 1, 2, 4, 8 where replicas are few) on the
+ * handle's own systems, restores the state after every probe, and keeps the
+ * fastest. Outputs (may be NULL): the chosen
  * threads, layout and probe time in ms. No reference counterpart (the
  * reference fixes its block size by system size, main.cpp:1746-1747). */
 int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads,
                   int* mol_in_smem, float* best_ms);
 /* Set the sweep schedule directly (threads 32, 64, 128 or 256). */
 int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem);
+/* CTAs per replica: 1, or a thread-block cluster of 2, 4 or 8 CTAs that share
+ * each replica's pair loops (for batches with fewer replicas than SMs). The
+ * autotuner also tries clusters when n_inst * size <= 2 * SMs. No reference
+ * counterpart. */
+int remc_set_cluster(remc_handle* h, int cluster);
+int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* cluster);
 
 int remc_sync(remc_handle* h);
 int remc_num_instances(const remc_handle* h);

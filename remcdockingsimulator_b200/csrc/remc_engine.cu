@@ -24,6 +24,7 @@
 //                      CudaFunctions.cu:455-685).
 //   exchange_kernel    one warp per system, disjoint temperature pairs in
 //                      parallel lanes (main.cpp:1427-1453).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -207,7 +208,8 @@ struct SweepArgs {
   int rec_stride, rec_offset;       // records of step s at rec_offset + s
   int n_steps;
   int nmax, mmax, lmax;  // shared-memory capacities
-  int mol_in_smem;       // centres and molecule starts resident in shared memory
+  int mol_in_smem;       // centres resident in shared memory
+  int csize;             // CTAs per replica (a thread-block cluster), 1, 2, 4 or 8
   EnergyConsts K;
 };
 
@@ -216,7 +218,7 @@ constexpr int kRing = 64;  // proposal records held in shared memory (two halves
 // Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
 // mmax molecules, lmax beads per molecule).
 struct SweepSmem {
-  size_t tab, beads, centres, trial_pos, ring, red, total;
+  size_t tab, beads, centres, trial_pos, trial_rel, ring, red, total;
   static __host__ __device__ size_t take(size_t& off, size_t bytes) {
     size_t o = off;
     off += (bytes + 15) & ~size_t(15);
@@ -224,15 +226,17 @@ struct SweepSmem {
   }
   // mol_in_smem = 0: molecule centres and starts stay in global memory (the
   // largest systems), everything else as usual
-  static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax, int mol_in_smem) {
+  static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax, int mol_in_smem,
+                                            int csize = 1) {
     SweepSmem s;
     size_t off = 0;
     s.tab = take(off, sizeof(float4) * kNT * kNT);
     s.beads = take(off, sizeof(float4) * nmax);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
+    s.trial_rel = take(off, sizeof(float4) * lmax);
     s.ring = take(off, sizeof(StepRec) * kRing);
-    s.red = take(off, sizeof(double) * 2 * 2 * 32);
+    s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
     return s;
   }
@@ -265,20 +269,35 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the trial buffer rather than from another thread's not-yet-ordered write.
 // A step of a one-bead molecule therefore costs one barrier; a chain step
 // costs two (trial positions are built by the owners of the chain's beads).
-template <bool R12, bool CUT>
+template <bool R12, bool CUT, bool CLUSTER>
 __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem);
+  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem, A.csize);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
   float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
   float4* s_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
+  // rotated relative positions of the chain's beads, computed with its trial
+  // positions by the beads' owners and installed by the same threads: the
+  // install writes rel without reading it, so the CTAs of a cluster, which
+  // all install the same values, cannot read one another's update
+  float4* s_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
   StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
 
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int tmask = nthr - 1;  // nthr is a power of two
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+  // A replica may span a cluster of csize CTAs: every CTA holds the whole
+  // replica and runs every step, the pair loops split bead j over the
+  // cluster's threads (CTA rank r, thread t takes j = r T + t mod csize T;
+  // within a CTA that is still j = t mod T, so ownership is unchanged), the
+  // warps' partial sums go to every CTA's shared memory, and one cluster
+  // barrier per step replaces the CTA barrier. Rank 0 alone writes state that
+  // is not idempotent (rotations, counters, samples) and the final state.
+  const int csize = CLUSTER ? A.csize : 1;
+  const int crank = CLUSTER ? (int)cooperative_groups::this_cluster().block_rank() : 0;
+  const int gtid = crank * nthr + tid, gstride = nthr * csize, gmask = gstride - 1;
   __shared__ int s_next;
   for (int it = 0;; ++it) {
   int idx;
@@ -290,7 +309,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     if (idx >= A.n_list) break;
   } else {
     if (it > 0) break;
-    idx = blockIdx.x;
+    idx = blockIdx.x / csize;
   }
   const int inst = A.inst_list[idx];
   const int sysid = A.inst_sys[inst];
@@ -331,7 +350,11 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   const uint32_t step0 = A.ctrl ? A.ctrl[0] : A.step0;
   int to_sample = A.sample_every;  // steps left in the current sampling chunk
   __shared__ long long s_pose_slot;
-  __syncthreads();
+  // every CTA of a cluster has started before any writes another's shared memory
+  if (CLUSTER)
+    cooperative_groups::this_cluster().sync();
+  else
+    __syncthreads();
   // centre of the next step's molecule when centres live in global memory
   float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f);
   if (n_steps > 0 && !A.mol_in_smem) next_c = cent[s_ring[0].m];
@@ -405,6 +428,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         if (rec.rotate) {
           const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
           np = make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
+          s_trel[k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
         } else {
           np = make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
         }
@@ -429,9 +453,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           const int lo = part ? x1 : 0, hi = part ? N : x0;
           if (lo >= hi) continue;
           const int cb = min(hi, ncb);
-          int j = lo + ((tid - lo) & tmask);  // first j >= lo with j = tid (mod T)
+          int j = lo + ((gtid - lo) & gmask);  // first j >= lo in this thread's class
           if (!rec.crowd) {
-            for (; j < cb; j += nthr) {
+            for (; j < cb; j += gstride) {
               const float4 pj = s_beads[j];
               const float4 Tj = trow[bead_type(pj.w)];
               const float en = pair_energy_r2(pair_r2(pnew1, pj, box, invbox), Tj, false, A.K);
@@ -439,7 +463,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               acc_c += en - eo;
             }
           } else {
-            for (; j < cb; j += nthr) {
+            for (; j < cb; j += gstride) {
               const float4 pj = s_beads[j];
               const float4 Tj = trow[bead_type(pj.w)];
               const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
@@ -448,7 +472,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             }
           }
           const float4 Tc = trow[ctype >= 0 ? ctype : 0];
-          for (; j < hi; j += nthr) {
+          for (; j < hi; j += gstride) {
             const float4 pj = s_beads[j];
             const float4 Tj = ctype >= 0 ? Tc : trow[bead_type(pj.w)];
             const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
@@ -465,8 +489,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           const int lo = part ? x1 : 0, hi = part ? N : x0;
           if (lo >= hi) continue;
           const int cb = min(hi, ncb);
-          int j = lo + ((tid - lo) & tmask);
-          for (; j < cb; j += nthr) {
+          int j = lo + ((gtid - lo) & gmask);
+          for (; j < cb; j += gstride) {
             const float4 pj = s_beads[j];
             const int tb = bead_type(pj.w);
             float a = 0.0f;
@@ -490,7 +514,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               acc_o += a;
             }
           }
-          for (; j < hi; j += nthr) {
+          for (; j < hi; j += gstride) {
             const float4 pj = s_beads[j];
             const int tb = bead_type(pj.w);
             float a = 0.0f;
@@ -511,11 +535,24 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     dacc = warp_sum(dacc);
     if (!rec.crowd) dcc = warp_sum(dcc);
     if (lane == 0) {
-      s_red[b * 64 + warp] = dacc;
-      s_red[b * 64 + 32 + warp] = dcc;
+      if (!CLUSTER) {
+        s_red[b * 64 + warp] = dacc;
+        s_red[b * 64 + 32 + warp] = dcc;
+      } else {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        for (int r = 0; r < csize; ++r) {
+          double* dst = cl.map_shared_rank(s_red, r) + (b * csize + crank) * 64;
+          dst[warp] = dacc;
+          dst[32 + warp] = dcc;
+        }
+      }
     }
     if ((s & 31) == 31) cp_async_wait_all();  // next ring half has landed
-    __syncthreads();  // R: partial sums (and the prefetched records) visible
+    // R: partial sums (and the prefetched records) visible
+    if (!CLUSTER)
+      __syncthreads();
+    else
+      cooperative_groups::this_cluster().sync();
 
     // ---- every thread: the same FP64 sums (a fixed pairwise tree over the
     // warps' partials) and the same Metropolis decision
@@ -525,12 +562,14 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       // from registers instead (same && !p_rot)
       next_c = cent[s_ring[(s + 1) & (kRing - 1)].m];
     }
-    double dE = tree_sum8(s_red + b * 64, nwarps);
+    double dE = tree_sum8(s_red + b * csize * 64, nwarps);
     double dE_cc = 0.0;
-    if (!rec.crowd) {
-      dE_cc = tree_sum8(s_red + b * 64 + 32, nwarps);
-      dE += dE_cc;
+    if (!rec.crowd) dE_cc = tree_sum8(s_red + b * csize * 64 + 32, nwarps);
+    for (int r = 1; r < csize; ++r) {  // the other CTAs' sums, in rank order
+      dE += tree_sum8(s_red + (b * csize + r) * 64, nwarps);
+      if (!rec.crowd) dE_cc += tree_sum8(s_red + (b * csize + r) * 64 + 32, nwarps);
     }
+    if (!rec.crowd) dE += dE_cc;
     const int acc = dE < 0.0 ? 1 : (dE < recs_.thr ? 2 : 0);
     if (acc) {
       energy += dE;
@@ -540,21 +579,16 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         p_single = pnew1;
       } else {
         // the owners install the chain (and its relative positions)
-        QuatProducts qp{};
-        if (rec.rotate) qp = quat_products(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3]);
         int j = m0 + ((tid - m0) & tmask);
         for (; j < m0 + n; j += nthr) {
           s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
-          if (rec.rotate) {
-            const float4 rl = A.rel[bead_off + j];
-            const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
-            A.rel[bead_off + j] = make_float4(r2.x, r2.y, r2.z, 0.0f);
-          }
+          if (rec.rotate) A.rel[bead_off + j] = s_trel[j - m0];
         }
       }
       if (tid == 0) {
         if (acc == 1) ++n_neg; else ++n_boltz;
         if (rec.rotate) {
+          if (crank == 0) {
           double* qd = A.quat + 4 * (size_t)(mol_off + m);
           double out[4];
           quat_mul(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3], qd[0], qd[1], qd[2], qd[3], out);
@@ -562,6 +596,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           qd[1] = out[1];
           qd[2] = out[2];
           qd[3] = out[3];
+          }
         } else {
           cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
         }
@@ -591,7 +626,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           ++n_samp;
           n_bnd += bound ? 1 : 0;
         }
-        if (bound && A.sample_out) {
+        if (bound && A.sample_out && crank == 0) {
           __syncthreads();  // this step's centre / rotation writes visible
           if (tid == 0) {
             const unsigned r = atomicAdd(&A.sample_cursor[0], 1u);
@@ -647,11 +682,14 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   (void)p_n;
   __syncthreads();
 
-  // ---- epilogue: write the instance back
+  // ---- epilogue: write the instance back (every CTA of a cluster holds the
+  // same state; rank 0 writes it)
+  if (crank == 0) {
   for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
   if (A.mol_in_smem)
     for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
-  if (tid == 0) {
+  }
+  if (tid == 0 && crank == 0) {
     A.energy[inst] = energy;
     A.ecc[inst] = ecc;
     A.n_samples[inst] += n_samp;
@@ -664,6 +702,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   }
   __syncthreads();  // shared memory is reused by the next instance
   }  // instance loop
+  // no CTA leaves while another may still write into its shared memory
+  if (CLUSTER) cooperative_groups::this_cluster().sync();
 }
 
 // ------------------------------------------------------------------ full E
@@ -1226,6 +1266,7 @@ struct remc_handle {
   int* d_queue = nullptr;
   int sweep_grid = 0;  // resident CTAs of the persistent sweep
   int mol_in_smem = 1; // molecule centres/starts in shared memory (else global)
+  int sweep_csize = 1; // CTAs per replica (thread-block cluster size)
   int max_dyn_smem = 0;
   int config_gen = 0;  // bumped when the sweep schedule changes
   TileItem* d_items = nullptr;
@@ -1364,31 +1405,59 @@ int ensure_recs(remc_handle* h, size_t steps) {
   return REMC_OK;
 }
 
-// The sweep kernel compiled for the handle's crowder model.
+// The sweep kernel compiled for the handle's crowder model, single CTAs or
+// clusters of CTAs per replica.
 using SweepFn = void (*)(SweepArgs);
-SweepFn sweep_fn(const remc_params& p) {
+SweepFn sweep_fn(const remc_params& p, bool cluster) {
   const bool cut = p.crowder_cutoff > 0.0f;
-  if (p.crowder_mode) return cut ? sweep_kernel<true, true> : sweep_kernel<true, false>;
-  return cut ? sweep_kernel<false, true> : sweep_kernel<false, false>;
+  if (cluster) {
+    if (p.crowder_mode) return cut ? sweep_kernel<true, true, true> : sweep_kernel<true, false, true>;
+    return cut ? sweep_kernel<false, true, true> : sweep_kernel<false, false, true>;
+  }
+  if (p.crowder_mode) return cut ? sweep_kernel<true, true, false> : sweep_kernel<true, false, false>;
+  return cut ? sweep_kernel<false, true, false> : sweep_kernel<false, false, false>;
 }
 
 // Set the sweep schedule: threads per replica and where molecule data lives.
-int configure_sweep(remc_handle* h, int threads, int mol_in_smem) {
+int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize) {
   if (threads < 32 || threads > 256 || (threads & (threads - 1)) != 0)
     return set_error(REMC_ERR_INVALID, "threads per replica must be 32, 64, 128 or 256");
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem).total;
+  if (csize != 1 && csize != 2 && csize != 4 && csize != 8)
+    return set_error(REMC_ERR_INVALID, "cluster size must be 1, 2, 4 or 8");
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem, csize).total;
   if (smem > (size_t)h->max_dyn_smem)
     return set_error(REMC_ERR_INVALID,
                      "largest system needs %zu bytes of shared memory, device allows %d", smem,
                      h->max_dyn_smem);
   int per_sm = 0;
   cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_fn(h->params), threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_fn(h->params, csize > 1), threads,
+                                                    smem);
   if (e != cudaSuccess || per_sm < 1)
     return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
                      cudaGetErrorString(e));
+  if (csize > 1) {
+    // the cluster must be schedulable: csize CTAs of this size in one GPC
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(csize);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, sweep_fn(h->params, true), &cfg);
+    if (e != cudaSuccess || clusters < 1)
+      return set_error(REMC_ERR_INVALID, "a cluster of %d sweep CTAs does not fit: %s", csize,
+                       cudaGetErrorString(e));
+  }
   h->sweep_threads = threads;
   h->mol_in_smem = mol_in_smem;
+  h->sweep_csize = csize;
   h->sweep_grid = per_sm * h->num_sms;
   h->config_gen++;
   return REMC_OK;
@@ -1434,8 +1503,13 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.sys = h->d_sys;
   A.inst_sys = h->d_inst_sys;
   A.inst_list = inst_list;
+  // a cluster schedule runs one cluster per replica (no work queue); the
+  // one-replica-per-launch path always runs single CTAs
+  const int csize = persistent ? h->sweep_csize : 1;
+  if (csize > 1) persistent = false;
   A.queue = persistent ? h->d_queue : nullptr;
   A.n_list = n_blocks;
+  A.csize = csize;
   if (persistent) {
     REMC_CUDA_TRY(cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->stream));
     n_blocks = std::min(n_blocks, h->sweep_grid);
@@ -1476,8 +1550,24 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.mol_in_smem = h->mol_in_smem;
   A.lmax = h->lmax;
   A.K = consts_of(h);
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem).total;
-  sweep_fn(h->params)<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
+  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem, csize).total;
+  if (csize == 1) {
+    sweep_fn(h->params, false)<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(csize * n_blocks);
+    cfg.blockDim = dim3(h->sweep_threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    REMC_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_fn(h->params, true), A));
+  }
   REMC_CUDA_TRY(cudaGetLastError());
   return REMC_OK;
 }
@@ -1625,8 +1715,11 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   int max_smem = 0;
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  const SweepFn kSweeps[4] = {sweep_kernel<false, false>, sweep_kernel<false, true>,
-                              sweep_kernel<true, false>, sweep_kernel<true, true>};
+  const SweepFn kSweeps[8] = {
+      sweep_kernel<false, false, false>, sweep_kernel<false, true, false>,
+      sweep_kernel<true, false, false>,  sweep_kernel<true, true, false>,
+      sweep_kernel<false, false, true>,  sweep_kernel<false, true, true>,
+      sweep_kernel<true, false, true>,   sweep_kernel<true, true, true>};
   int static_smem = 0;
   for (SweepFn f : kSweeps) {
     cudaFuncAttributes fattr;
@@ -1650,8 +1743,8 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   // memory when it fits, more threads per replica for larger systems
   {
     const int threads = h->nmax <= 2048 ? 128 : 256;
-    int rc0 = configure_sweep(h, threads, 1);
-    if (rc0) rc0 = configure_sweep(h, threads, 0);
+    int rc0 = configure_sweep(h, threads, 1, 1);
+    if (rc0) rc0 = configure_sweep(h, threads, 0, 1);
     if (rc0) {
       delete h;
       return rc0;
@@ -2378,14 +2471,20 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   h->sample_every = 0;
   rc = ensure_recs(h, (size_t)probe_steps);
   const int cand_threads[2] = {128, 256};
-  int best_t = h->sweep_threads, best_m = h->mol_in_smem;
+  // clusters of CTAs per replica only pay when replicas are fewer than the
+  // CTAs the GPU can hold
+  int cand_c[4] = {1, 0, 0, 0}, n_c = 1;
+  for (int c = 2; c <= 8; c *= 2)
+    if ((long long)h->n_inst * c <= 2LL * h->num_sms) cand_c[n_c++] = c;
+  int best_t = h->sweep_threads, best_m = h->mol_in_smem, best_c = h->sweep_csize;
   float best = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  for (int ci = 0; ci < n_c && !rc; ++ci) {
   for (int ti = 0; ti < 2 && !rc; ++ti) {
     for (int mi = 1; mi >= 0 && !rc; --mi) {
-      if (configure_sweep(h, cand_threads[ti], mi) != REMC_OK) continue;
+      if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci]) != REMC_OK) continue;
       float ms = 0.0f;
       for (int rep = 0; rep < 2 && !rc; ++rep) {  // first launch warms up
         cudaEventRecord(e0, h->stream);
@@ -2403,8 +2502,10 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
         best = ms;
         best_t = cand_threads[ti];
         best_m = mi;
+        best_c = cand_c[ci];
       }
     }
+  }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2412,7 +2513,7 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   cudaStreamSynchronize(h->stream);
   release();
   if (rc) return rc;
-  rc = configure_sweep(h, best_t, best_m);
+  rc = configure_sweep(h, best_t, best_m, best_c);
   if (rc) return rc;
   if (threads_out) *threads_out = best_t;
   if (mol_in_smem_out) *mol_in_smem_out = best_m;
@@ -2423,7 +2524,21 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
 int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return configure_sweep(h, threads, mol_in_smem ? 1 : 0);
+  return configure_sweep(h, threads, mol_in_smem ? 1 : 0, h->sweep_csize);
+}
+
+int remc_set_cluster(remc_handle* h, int cluster) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return configure_sweep(h, h->sweep_threads, h->mol_in_smem, cluster);
+}
+
+int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* cluster) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (threads) *threads = h->sweep_threads;
+  if (mol_in_smem) *mol_in_smem = h->mol_in_smem;
+  if (cluster) *cluster = h->sweep_csize;
+  return REMC_OK;
 }
 
 int remc_sync(remc_handle* h) {

@@ -326,6 +326,16 @@ class Engine:
                                   C.byref(ms)))
         return t.value, bool(m.value), ms.value
 
+    def set_cluster(self, cluster: int) -> None:
+        """CTAs per replica (a thread-block cluster of 1, 2, 4 or 8)."""
+        check(lib().remc_set_cluster(self._h, cluster))
+
+    def schedule(self):
+        """(threads per replica, centres in shared memory, CTAs per replica)."""
+        t, m, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().remc_get_schedule(self._h, C.byref(t), C.byref(m), C.byref(c)))
+        return t.value, bool(m.value), c.value
+
     def set_schedule(self, threads: int, mol_in_smem: bool) -> None:
         check(lib().remc_set_schedule(self._h, threads, 1 if mol_in_smem else 0))
 

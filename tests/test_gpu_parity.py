@@ -85,7 +85,7 @@ def test_delta_energy_api_vs_oracle(built_lib):
             assert abs(d_gpu - d_ref) <= E_RTOL * max(scale, 1e-3), (m, d_gpu, d_ref)
 
 
-def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None):
+def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None, cluster=1):
     from oracle import bindings as ob
     s = w.systems[0]
     lad = w.ladders[0][:R]
@@ -93,6 +93,9 @@ def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None)
     rs = np.full(R, w.rotate_step) if rsteps is None else rsteps
     with _engine([s], R, w.params) as eng:
         eng.set_replica_params([lad], ts, rs)
+        if cluster > 1:
+            eng.set_cluster(cluster)
+            assert eng.schedule()[2] == cluster
         e0 = eng.energy_full()
         eng.sweep(n_steps, seed, step0)
         e_run = eng.energies()
@@ -130,6 +133,18 @@ def test_sweep_crowded_vs_oracle(built_lib):
     from remcdockingsimulator_b200 import synth
     w = synth.crowded(7)
     _run_sweep_vs_oracle(w, 3, 1500, seed=77)
+
+
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+def test_sweep_cluster_vs_oracle(cluster, built_lib):
+    """A replica spread over a cluster of CTAs (pair loops split over the
+    cluster, partial sums exchanged through distributed shared memory) follows
+    the oracle's trajectory like a single CTA does."""
+    from remcdockingsimulator_b200 import synth
+    w = synth.crowded(7)
+    _run_sweep_vs_oracle(w, 3, 1500, seed=77, cluster=cluster)
+    w2 = synth.two_chain(7)
+    _run_sweep_vs_oracle(w2, 2, 800, seed=5, cluster=cluster)
 
 
 def test_sweep_crowded_reference_mode_rotating_crowders(built_lib):
@@ -215,9 +230,11 @@ def test_exchange_vs_oracle(built_lib):
             eng.sweep(100, 1, 300 + 100 * rnd)
 
 
-def test_graph_run_matches_stepwise(built_lib):
+@pytest.mark.parametrize("cluster", [1, 4])
+def test_graph_run_matches_stepwise(cluster, built_lib):
     """remc_run (captured graph, device-side counters) == explicit
-    sweep/exchange calls with the same counters."""
+    sweep/exchange calls with the same counters (single CTAs, and clusters
+    launched inside the captured graph)."""
     from remcdockingsimulator_b200 import synth
     w = synth.crowded(9)
     s = w.systems[0]
@@ -228,6 +245,8 @@ def test_graph_run_matches_stepwise(built_lib):
         with _engine([s, s], [R, R], w.params) as eng:
             eng.set_replica_params([lad, lad], np.full(2 * R, 0.5, np.float32),
                                    np.full(2 * R, 0.2))
+            if cluster > 1:
+                eng.set_cluster(cluster)
             eng.energy_full()
             if graph:
                 eng.run(5, 200, 4242, 0, 0)

@@ -22,8 +22,8 @@ def _oracle_chunks(o, s, state, T, ts, rs, seed, slot, n_steps, f, e0, thr):
     return out, state, E
 
 
-@pytest.mark.parametrize("name", ["crowded", "two_chain"])
-def test_sampling_counts_and_bound_decisions(name, built_lib):
+@pytest.mark.parametrize("name,cluster", [("crowded", 1), ("two_chain", 1), ("crowded", 4)])
+def test_sampling_counts_and_bound_decisions(name, cluster, built_lib):
     from oracle import bindings as ob
     from remcdockingsimulator_b200 import synth
     from remcdockingsimulator_b200.engine import Engine
@@ -40,6 +40,8 @@ def test_sampling_counts_and_bound_decisions(name, built_lib):
     thr = float(np.median([p[0] for p in probe]))
     with Engine([s], R, w.params) as eng:
         eng.set_replica_params([lad], np.full(R, 0.5, np.float32), np.full(R, 0.2))
+        if cluster > 1:
+            eng.set_cluster(cluster)  # rank 0 of each cluster writes the samples
         e0 = eng.energy_full()
         assert abs(eng.noncrowder_energies()[0] - ecc0) <= E_RTOL * max(abs(ecc0), 1e-3)
         eng.set_sampling(f, 0, thr, max_records=R * n // f, max_poses=R * n // f * s.n_mol)
