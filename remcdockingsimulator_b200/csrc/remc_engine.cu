@@ -706,6 +706,67 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   if (CLUSTER) cooperative_groups::this_cluster().sync();
 }
 
+// ------------------------------------------------------------------ state staging
+// Host layout (3 floats per bead and molecule) <-> device layout (float4 with
+// the bead meta word), converted on the device so that uploads and downloads
+// are plain copies of the caller's buffers.
+__global__ void state_check_kernel(const float* __restrict__ pos3, const float* __restrict__ rel3,
+                                   const float* __restrict__ cen3, const int* __restrict__ info,
+                                   long long nb, long long nm,
+                                   unsigned long long* __restrict__ bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb; i += stride) {
+    const float* p = pos3 + 3 * i;
+    const float* r = rel3 + 3 * i;
+    bool fin = true;
+    for (int k = 0; k < 3; ++k) fin = fin && isfinite(p[k]) && isfinite(r[k]);
+    if (!fin) atomicMin(&bad[0], (unsigned long long)i);
+    if ((info[i] & (int)0x80000000u) && (r[0] != 0.0f || r[1] != 0.0f || r[2] != 0.0f))
+      atomicMin(&bad[1], (unsigned long long)i);
+  }
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < nm; m += stride) {
+    const float* c = cen3 + 3 * m;
+    if (!(isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2])))
+      atomicMin(&bad[2], (unsigned long long)m);
+  }
+}
+
+__global__ void state_pack_kernel(const float* __restrict__ pos3, const float* __restrict__ rel3,
+                                  const float* __restrict__ cen3, const int* __restrict__ info,
+                                  long long nb, long long nm, float4* __restrict__ pos,
+                                  float4* __restrict__ rel, float4* __restrict__ cen) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb; i += stride) {
+    pos[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2],
+                         __int_as_float(info[i] & 0x7fffffff));
+    rel[i] = make_float4(rel3[3 * i], rel3[3 * i + 1], rel3[3 * i + 2], 0.0f);
+  }
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < nm; m += stride)
+    cen[m] = make_float4(cen3[3 * m], cen3[3 * m + 1], cen3[3 * m + 2], 0.0f);
+}
+
+__global__ void state_unpack_kernel(const float4* __restrict__ pos, const float4* __restrict__ rel,
+                                    const float4* __restrict__ cen, long long nb, long long nm,
+                                    float* __restrict__ pos3, float* __restrict__ rel3,
+                                    float* __restrict__ cen3) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb; i += stride) {
+    const float4 p = pos[i], r = rel[i];
+    pos3[3 * i] = p.x;
+    pos3[3 * i + 1] = p.y;
+    pos3[3 * i + 2] = p.z;
+    rel3[3 * i] = r.x;
+    rel3[3 * i + 1] = r.y;
+    rel3[3 * i + 2] = r.z;
+  }
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < nm; m += stride) {
+    const float4 c = cen[m];
+    cen3[3 * m] = c.x;
+    cen3[3 * m + 1] = c.y;
+    cen3[3 * m + 2] = c.z;
+  }
+}
+
 // ------------------------------------------------------------------ full E
 struct TileItem {
   int inst, ti, tj, pad;
@@ -1292,6 +1353,10 @@ struct remc_handle {
   int n_items = 0;
   float4* d_newpos = nullptr;
   double* d_dE = nullptr;
+  int* d_bead_info = nullptr;  // per bead per instance: meta word | (one-bead molecule << 31)
+  float* d_stage = nullptr;    // host-layout staging: pos[3n], rel[3n], centre[3m]
+  double* d_stage_q = nullptr; // quaternions [4m]
+  unsigned long long* d_bad = nullptr;  // first invalid bead / one-bead offset / molecule
   int sweep_threads = 128;
   int num_sms = 148;
   // graph
@@ -1325,7 +1390,7 @@ void free_all(remc_handle* h) {
                   h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_forces, h->d_G,
                   h->d_dxi,        h->d_eadj,     h->d_mft,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
-                  h->d_dE};
+                  h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1788,6 +1853,10 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_inst_sys, h->n_inst);
   if (!rc) rc = dev_alloc(&h->d_inst_list, h->n_inst);
   if (!rc) rc = dev_alloc(&h->d_pos, h->total_beads);
+  if (!rc) rc = dev_alloc(&h->d_bead_info, h->total_beads);
+  if (!rc) rc = dev_alloc(&h->d_stage, 6 * h->total_beads + 3 * h->total_mols);
+  if (!rc) rc = dev_alloc(&h->d_stage_q, 4 * h->total_mols);
+  if (!rc) rc = dev_alloc(&h->d_bad, 3);
   if (!rc) rc = dev_alloc(&h->d_rel, h->total_beads);
   if (!rc) rc = dev_alloc(&h->d_centre, h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_quat, 4 * h->total_mols);
@@ -1838,6 +1907,21 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   up(h->d_mrole_off, mrole_off.data(), sizeof(int) * h->n_sys);
   up(h->d_items, items.data(), sizeof(TileItem) * items.size());
   up(h->d_item_off, item_off.data(), sizeof(int) * item_off.size());
+  // per bead per instance: the meta word of pos.w, and bit 31 for beads of
+  // one-bead molecules (whose relative position must be zero)
+  std::vector<int> bead_info(h->total_beads);
+  for (int g = 0; g < h->n_inst; ++g) {
+    const int s2 = h->h_inst_sys[g];
+    const SysDev& S = h->h_sys[s2];
+    const size_t b0 = (size_t)S.bead_base + (size_t)(g - S.inst0) * S.n_beads;
+    const int* ms = &h->h_mol_start[S.mstart_off];
+    const int* bt = &h->h_bead_type[h->h_bead_off_static[s2]];
+    for (int m = 0; m < S.n_mol; ++m)
+      for (int b = ms[m]; b < ms[m + 1]; ++b)
+        bead_info[b0 + b] =
+            pack_meta(m, bt[b]) | (ms[m + 1] - ms[m] == 1 ? (int)0x80000000u : 0);
+  }
+  up(h->d_bead_info, bead_info.data(), sizeof(int) * bead_info.size());
   if (!rc) {
     cudaMemsetAsync(h->d_acc_neg, 0, sizeof(int) * h->n_inst, h->stream);
     cudaMemsetAsync(h->d_acc_boltz, 0, sizeof(int) * h->n_inst, h->stream);
@@ -1898,48 +1982,53 @@ int remc_set_type_tables(remc_handle* h, const float* vdw, const float* charge, 
 int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const float* centre,
                       const double* quat) {
   if (!h || !pos || !rel || !centre || !quat) return set_error(REMC_ERR_INVALID, "null argument");
-  std::vector<float4> p(h->total_beads), r(h->total_beads), c(h->total_mols);
-  for (int g = 0; g < h->n_inst; ++g) {
-    const int s = h->h_inst_sys[g];
-    const SysDev& S = h->h_sys[s];
-    const int slot = g - S.inst0;
-    const size_t b0 = (size_t)S.bead_base + (size_t)slot * S.n_beads;
-    const size_t m0 = (size_t)S.mol_base + (size_t)slot * S.n_mol;
-    const int* ms = &h->h_mol_start[S.mstart_off];
-    const int* bt = &h->h_bead_type[h->h_bead_off_static[s]];
-    for (int m = 0; m < S.n_mol; ++m) {
-      const size_t gm = m0 + m;
-      for (int k = 0; k < 3; ++k)
-        if (!std::isfinite(centre[3 * gm + k]))
-          return set_error(REMC_ERR_NUMERIC, "instance %d molecule %d: non-finite centre", g, m);
-      c[gm] = make_float4(centre[3 * gm], centre[3 * gm + 1], centre[3 * gm + 2], 0.0f);
-      for (int b = ms[m]; b < ms[m + 1]; ++b) {
-        const size_t gb = b0 + b;
-        for (int k = 0; k < 3; ++k)
-          if (!std::isfinite(pos[3 * gb + k]) || !std::isfinite(rel[3 * gb + k]))
-            return set_error(REMC_ERR_NUMERIC, "instance %d bead %d: non-finite coordinate", g, b);
-        int meta = pack_meta(m, bt[b]);
-        float w;
-        memcpy(&w, &meta, sizeof(w));
-        p[gb] = make_float4(pos[3 * gb], pos[3 * gb + 1], pos[3 * gb + 2], w);
-        r[gb] = make_float4(rel[3 * gb], rel[3 * gb + 1], rel[3 * gb + 2], 0.0f);
-        if (ms[m + 1] - ms[m] == 1 && (rel[3 * gb] != 0.0f || rel[3 * gb + 1] != 0.0f ||
-                                       rel[3 * gb + 2] != 0.0f))
-          return set_error(REMC_ERR_INVALID,
-                           "instance %d molecule %d: a one-bead molecule must sit at its centre",
-                           g, m);
-      }
-    }
-  }
-  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_pos, p.data(), sizeof(float4) * p.size(),
+  const size_t nb = h->total_beads, nm = h->total_mols;
+  float* sp = h->d_stage;
+  float* sr = sp + 3 * nb;
+  float* sc = sr + 3 * nb;
+  // the caller's buffers go to staging as they are; the state changes only
+  // after every coordinate has been checked
+  REMC_CUDA_TRY(cudaMemcpyAsync(sp, pos, sizeof(float) * 3 * nb, cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(sr, rel, sizeof(float) * 3 * nb, cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(sc, centre, sizeof(float) * 3 * nm, cudaMemcpyHostToDevice,
+                                h->stream));
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_stage_q, quat, sizeof(double) * 4 * nm,
                                 cudaMemcpyHostToDevice, h->stream));
-  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_rel, r.data(), sizeof(float4) * r.size(),
-                                cudaMemcpyHostToDevice, h->stream));
-  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_centre, c.data(), sizeof(float4) * c.size(),
-                                cudaMemcpyHostToDevice, h->stream));
-  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_quat, quat, sizeof(double) * 4 * h->total_mols,
-                                cudaMemcpyHostToDevice, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_bad, 0x7f, sizeof(unsigned long long) * 3, h->stream));
+  const int grid = h->num_sms * 4;
+  state_check_kernel<<<grid, 256, 0, h->stream>>>(sp, sr, sc, h->d_bead_info, (long long)nb,
+                                                  (long long)nm, h->d_bad);
+  REMC_CUDA_TRY(cudaGetLastError());
+  unsigned long long bad[3];
+  REMC_CUDA_TRY(cudaMemcpyAsync(bad, h->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const unsigned long long none = 0x7f7f7f7f7f7f7f7full;
+  if (bad[0] != none || bad[1] != none || bad[2] != none) {
+    // name the instance and bead / molecule of the first offender
+    for (int g = 0; g < h->n_inst; ++g) {
+      const SysDev& S = h->h_sys[h->h_inst_sys[g]];
+      const unsigned long long b0 =
+          (unsigned long long)S.bead_base + (unsigned long long)(g - S.inst0) * S.n_beads;
+      const unsigned long long m0 =
+          (unsigned long long)S.mol_base + (unsigned long long)(g - S.inst0) * S.n_mol;
+      if (bad[2] != none && bad[2] >= m0 && bad[2] < m0 + S.n_mol)
+        return set_error(REMC_ERR_NUMERIC, "instance %d molecule %d: non-finite centre", g,
+                         (int)(bad[2] - m0));
+      if (bad[0] != none && bad[0] >= b0 && bad[0] < b0 + S.n_beads)
+        return set_error(REMC_ERR_NUMERIC, "instance %d bead %d: non-finite coordinate", g,
+                         (int)(bad[0] - b0));
+      if (bad[1] != none && bad[1] >= b0 && bad[1] < b0 + S.n_beads)
+        return set_error(REMC_ERR_INVALID,
+                         "instance %d bead %d: a one-bead molecule must sit at its centre", g,
+                         (int)(bad[1] - b0));
+    }
+    return set_error(REMC_ERR_INVALID, "invalid state");
+  }
+  state_pack_kernel<<<grid, 256, 0, h->stream>>>(sp, sr, sc, h->d_bead_info, (long long)nb,
+                                                 (long long)nm, h->d_pos, h->d_rel, h->d_centre);
+  REMC_CUDA_TRY(cudaGetLastError());
+  REMC_CUDA_TRY(cudaMemcpyAsync(h->d_quat, h->d_stage_q, sizeof(double) * 4 * nm,
+                                cudaMemcpyDeviceToDevice, h->stream));
   h->state_set = true;
   return REMC_OK;
 }
@@ -1947,35 +2036,27 @@ int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const 
 int remc_download_state(remc_handle* h, float* pos, float* rel, float* centre, double* quat) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->state_set) return set_error(REMC_ERR_STATE, "state not uploaded");
-  std::vector<float4> p(h->total_beads), r(h->total_beads), c(h->total_mols);
-  REMC_CUDA_TRY(cudaMemcpyAsync(p.data(), h->d_pos, sizeof(float4) * p.size(),
-                                cudaMemcpyDeviceToHost, h->stream));
-  REMC_CUDA_TRY(cudaMemcpyAsync(r.data(), h->d_rel, sizeof(float4) * r.size(),
-                                cudaMemcpyDeviceToHost, h->stream));
-  REMC_CUDA_TRY(cudaMemcpyAsync(c.data(), h->d_centre, sizeof(float4) * c.size(),
-                                cudaMemcpyDeviceToHost, h->stream));
+  const size_t nb = h->total_beads, nm = h->total_mols;
+  float* sp = h->d_stage;
+  float* sr = sp + 3 * nb;
+  float* sc = sr + 3 * nb;
+  state_unpack_kernel<<<h->num_sms * 4, 256, 0, h->stream>>>(h->d_pos, h->d_rel, h->d_centre,
+                                                             (long long)nb, (long long)nm, sp, sr,
+                                                             sc);
+  REMC_CUDA_TRY(cudaGetLastError());
+  if (pos)
+    REMC_CUDA_TRY(cudaMemcpyAsync(pos, sp, sizeof(float) * 3 * nb, cudaMemcpyDeviceToHost,
+                                  h->stream));
+  if (rel)
+    REMC_CUDA_TRY(cudaMemcpyAsync(rel, sr, sizeof(float) * 3 * nb, cudaMemcpyDeviceToHost,
+                                  h->stream));
+  if (centre)
+    REMC_CUDA_TRY(cudaMemcpyAsync(centre, sc, sizeof(float) * 3 * nm, cudaMemcpyDeviceToHost,
+                                  h->stream));
   if (quat)
-    REMC_CUDA_TRY(cudaMemcpyAsync(quat, h->d_quat, sizeof(double) * 4 * h->total_mols,
+    REMC_CUDA_TRY(cudaMemcpyAsync(quat, h->d_quat, sizeof(double) * 4 * nm,
                                   cudaMemcpyDeviceToHost, h->stream));
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  for (size_t i = 0; i < h->total_beads; ++i) {
-    if (pos) {
-      pos[3 * i] = p[i].x;
-      pos[3 * i + 1] = p[i].y;
-      pos[3 * i + 2] = p[i].z;
-    }
-    if (rel) {
-      rel[3 * i] = r[i].x;
-      rel[3 * i + 1] = r[i].y;
-      rel[3 * i + 2] = r[i].z;
-    }
-  }
-  if (centre)
-    for (size_t i = 0; i < h->total_mols; ++i) {
-      centre[3 * i] = c[i].x;
-      centre[3 * i + 1] = c[i].y;
-      centre[3 * i + 2] = c[i].z;
-    }
   return REMC_OK;
 }
 

@@ -194,13 +194,22 @@ class Engine:
         return out.value
 
     # ------------------------------------------------------------ read back
-    def download_state(self):
+    def download_state(self, out=None):
+        """(pos, rel, centre, quat) of every instance; `out` = four C-contiguous
+        arrays of those shapes and types to fill instead (e.g. pinned memory)."""
         nb = sum(s.n_beads * r for s, r in zip(self.systems, self.n_replicas))
         nm = sum(s.n_mol * r for s, r in zip(self.systems, self.n_replicas))
-        pos = np.zeros((nb, 3), np.float32)
-        rel = np.zeros((nb, 3), np.float32)
-        cen = np.zeros((nm, 3), np.float32)
-        quat = np.zeros((nm, 4), np.float64)
+        if out is not None:
+            pos, rel, cen, quat = out
+            for a, shape, dt in ((pos, (nb, 3), np.float32), (rel, (nb, 3), np.float32),
+                                 (cen, (nm, 3), np.float32), (quat, (nm, 4), np.float64)):
+                if a.shape != shape or a.dtype != dt or not a.flags.c_contiguous:
+                    raise ValueError("download_state: out arrays must be %s %s" % (shape, dt))
+        else:
+            pos = np.zeros((nb, 3), np.float32)
+            rel = np.zeros((nb, 3), np.float32)
+            cen = np.zeros((nm, 3), np.float32)
+            quat = np.zeros((nm, 4), np.float64)
         check(lib().remc_download_state(self._h, _ptr(pos, C.c_float), _ptr(rel, C.c_float),
                                         _ptr(cen, C.c_float), _ptr(quat, C.c_double)))
         return pos, rel, cen, quat

@@ -284,10 +284,18 @@ def test_bad_inputs_are_rejected(built_lib):
     s = w.systems[0]
     with _engine([s], 2, w.params) as eng:
         pos, rel, cen, quat = [np.concatenate([a, a]) for a in s.state()]
-        pos = pos.copy()
-        pos[3, 1] = np.nan
-        with pytest.raises(RemcError):
-            eng.upload_state(pos, rel, cen, quat)
+        before = eng.download_state()
+        bad = pos.copy()
+        bad[3, 1] = np.nan
+        with pytest.raises(RemcError, match="non-finite"):
+            eng.upload_state(bad, rel, cen, quat)
+        badc = cen.copy()
+        badc[1, 0] = np.inf
+        with pytest.raises(RemcError, match="centre"):
+            eng.upload_state(pos, rel, badc, quat)
+        # a refused upload leaves the state as it was
+        for a, b in zip(before, eng.download_state()):
+            assert np.array_equal(a, b)
         with pytest.raises(RemcError):
             eng.sweep(10, 1, 0)  # replica parameters not set yet
         with pytest.raises(RemcError):
