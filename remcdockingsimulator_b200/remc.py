@@ -65,6 +65,7 @@ class Args:
     resume: str = ""
     seed: Optional[int] = None
     sensitivity: bool = False
+    autotune: bool = False     # pick threads, layout and cluster size by probe sweeps
     checkpoint_every: int = 0  # MC steps between checkpoints (0: off)
     checkpoint_dir: str = "checkpoints"
     output_dir: str = "output"
@@ -146,6 +147,9 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
         elif t == "--sensitivity":
             a.sensitivity = True
             i += 1
+        elif t == "--autotune":
+            a.autotune = True
+            i += 1
         elif t == "--output-dir":
             a.output_dir = val()
             i += 2
@@ -161,7 +165,7 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
 
 USAGE = ("Usage: python -m remcdockingsimulator_b200 -f <filename> [-c] [-h] [-v] [-q] [-t x] "
          "[-s x] [-g x] [-m x] [-e x] [-r x] [-o x] [-b x] [-t0 x] [-t1 x] [-bx x] "
-         "[-z checkpoint] [--seed x] [--sensitivity] [--checkpoint-every steps] "
+         "[-z checkpoint] [--seed x] [--sensitivity] [--autotune] [--checkpoint-every steps] "
          "[--checkpoint-dir d] [--output-dir d] [--data-dir d]")
 
 _PLACE = re.compile(r"^([tp])\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*"
@@ -413,6 +417,12 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
     eng = Engine([system], R, params if params is not None else make_params())
     try:
         eng.set_replica_params([ladder], tsteps, rsteps)
+        if a.autotune:
+            # probe sweeps on a copy of the state; the state is restored after each
+            t, m, c = eng.autotune(probe_steps=min(256, max(1, a.mcsteps // a.resteps)))[:2] + \
+                (eng.schedule()[2],)
+            log("Autotuned sweep: %d threads per replica, molecule data in %s memory, "
+                "%d CTA(s) per replica" % (t, "shared" if m else "global", c))
         ck = load_simulation(a.resume) if a.resume else None
         if ck is None:
             e0 = eng.energy_full()

@@ -42,3 +42,8 @@ def test_checkpoint_layout_and_round_trip(tmp_path):
 def test_resume_flag_reads_config_and_pid(tmp_path):
     a = remc.parse_cli(["-z", "x/ck", "--checkpoint-every", "500"])
     assert a.resume == "x/ck" and a.checkpoint_every == 500
+
+
+def test_autotune_flag():
+    assert remc.parse_cli(["--autotune"]).autotune is True
+    assert remc.parse_cli([]).autotune is False
