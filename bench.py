@@ -63,6 +63,8 @@ def parse():
                     help="snapshots of the crowded system for the adjoint/energy cost ratio")
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MC steps of the per-replica-launch comparison sample")
+    ap.add_argument("--schedule", default="",
+                    help="THREADS,SMEM,CTAS: fixed sweep schedule instead of the autotuner")
     return ap.parse_args()
 
 
@@ -208,9 +210,17 @@ def main():
     eng.set_replica_params(w.ladders, np.full(len(w.systems), w.translate_step, np.float32),
                            np.full(len(w.systems), w.rotate_step))
     eng.energy_full()
-    # the project's autotuner picks threads per replica and the shared-memory
-    # layout for this batch (probe sweeps, state restored afterwards)
-    sched_threads, sched_smem, sched_ms = eng.autotune(probe_steps=min(args.block_steps, 256))
+    # the project's autotuner picks threads per replica, the shared-memory
+    # layout and CTAs per replica for this batch (probe sweeps, state restored
+    # afterwards), unless --schedule fixes them
+    if args.schedule:
+        t_, m_, c_ = (int(x) for x in args.schedule.split(","))
+        eng.set_schedule(t_, bool(m_))
+        eng.set_cluster(c_)
+        sched_threads, sched_smem, chosen_by = t_, bool(m_), "--schedule"
+    else:
+        sched_threads, sched_smem, _ = eng.autotune(probe_steps=min(args.block_steps, 256))
+        chosen_by = "remc_autotune"
     stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=torch.device("cuda", local))
     n_inst = eng.n_inst
     B = args.block_steps
@@ -388,7 +398,7 @@ def main():
                        "schedule": {"threads_per_replica": sched_threads,
                                     "molecule_data_in_shared_memory": sched_smem,
                                     "ctas_per_replica": eng.schedule()[2],
-                                    "chosen_by": "remc_autotune"},
+                                    "chosen_by": chosen_by},
                        "parallelism": "replicas" if world == 1 else "weak: %d independent batches" % world},
             "pair_energies_per_s": pair_evals_all / t_max,
             "pair_energy_note": "pair evaluations per second; a dE pair counts twice",

@@ -58,6 +58,47 @@ __device__ __forceinline__ float fast_ex2(float x) {
   return y;
 }
 
+// ---------------------------------------------------------------- bulk copies
+// One-dimensional TMA bulk copy global -> shared memory completed on an
+// mbarrier (no tensor map: the source is contiguous and 16-byte aligned, the
+// size a multiple of 16 bytes), without cluster multicast.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  // order this CTA's earlier generic-proxy reads of dst before the async write
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Wait for the mbarrier phase with the given parity to complete, at most
+// `limit` polls; returns false if it did not.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit) {
+  for (int i = 0; i < limit; ++i) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+        "selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------- energy
 struct EnergyConsts {
   float c_xi;        // -log2(e) / Xi: exp(-r/Xi) = ex2(r * c_xi)

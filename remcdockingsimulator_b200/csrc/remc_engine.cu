@@ -832,17 +832,25 @@ __device__ __forceinline__ void energy_row(const float4* __restrict__ s_j, int j
   }
 }
 
+// Polls of a bounded mbarrier wait (each poll may suspend the thread for a
+// while); reaching the limit means the copy never completed.
+constexpr int kWaitLimit = 1 << 22;
+
 __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
     const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
-    double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K) {
+    double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K,
+    int* __restrict__ err) {
   __shared__ float4 s_tab[kNT * kNT];
-  __shared__ float4 s_j[kTile];
+  __shared__ __align__(128) float4 s_j[kTile];
   __shared__ double s_red[kTile / 32];
   __shared__ double s_red_cc[kTile / 32];
+  __shared__ __align__(8) unsigned long long s_bar;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
+  if (tid == 0) mbar_init(&s_bar, 1);
+  unsigned phase = 0;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const TileItem W = items[it];
     const SysDev S = sys[inst_sys[W.inst]];
@@ -850,9 +858,15 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const int base = S.bead_base + (W.inst - S.inst0) * N;
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
-    __syncthreads();  // previous item done with s_j
-    if (tid < jn) s_j[tid] = pos[base + j0 + tid];
-    __syncthreads();
+    __syncthreads();  // previous item done with s_j (and the barrier initialised)
+    // the j-tile (contiguous, 16-byte aligned, 16 bytes per bead) by one bulk copy
+    if (tid == 0) bulk_load(s_j, pos + base + j0, 16u * (unsigned)jn, &s_bar);
+    const bool ok = mbar_wait(&s_bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {  // the copy never landed: report and stop
+      if (tid == 0) atomicOr(err, 1);
+      return;
+    }
     const int i = W.ti * kTile + tid;
     double dsum = 0.0, dcc = 0.0;
     if (i < N) {
@@ -1357,6 +1371,7 @@ struct remc_handle {
   float* d_stage = nullptr;    // host-layout staging: pos[3n], rel[3n], centre[3m]
   double* d_stage_q = nullptr; // quaternions [4m]
   unsigned long long* d_bad = nullptr;  // first invalid bead / one-bead offset / molecule
+  int* d_err = nullptr;        // set by a kernel whose bounded wait gave up
   int sweep_threads = 128;
   int num_sms = 148;
   // graph
@@ -1390,7 +1405,8 @@ void free_all(remc_handle* h) {
                   h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_forces, h->d_G,
                   h->d_dxi,        h->d_eadj,     h->d_mft,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
-                  h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad};
+                  h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad,
+                  h->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1444,6 +1460,18 @@ EnergyConsts consts_of(const remc_handle* h) {
   K.crowder_mode = h->params.crowder_mode;
   K.crowder_cut = h->params.crowder_cutoff > 0.0f ? 1 : 0;
   return K;
+}
+
+// Report (and clear) the error word a kernel sets when a bounded wait gives up.
+int check_device_error(remc_handle* h) {
+  int e = 0;
+  REMC_CUDA_TRY(cudaMemcpyAsync(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (e) {
+    REMC_CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+    return set_error(REMC_ERR_TIMEOUT, "a device-side wait for a bulk copy gave up");
+  }
+  return REMC_OK;
 }
 
 int check_ready(const remc_handle* h) {
@@ -1857,6 +1885,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_stage, 6 * h->total_beads + 3 * h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_stage_q, 4 * h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_bad, 3);
+  if (!rc) rc = dev_alloc(&h->d_err, 1);
   if (!rc) rc = dev_alloc(&h->d_rel, h->total_beads);
   if (!rc) rc = dev_alloc(&h->d_centre, h->total_mols);
   if (!rc) rc = dev_alloc(&h->d_quat, 4 * h->total_mols);
@@ -1932,6 +1961,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     cudaMemsetAsync(h->d_ex_acc, 0, sizeof(int) * h->n_sys, h->stream);
     cudaMemsetAsync(h->d_energy, 0, sizeof(double) * h->n_inst, h->stream);
     cudaMemsetAsync(h->d_ecc, 0, sizeof(double) * h->n_inst, h->stream);
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
     cudaMemsetAsync(h->d_n_samples, 0, sizeof(int) * h->n_inst, h->stream);
     cudaMemsetAsync(h->d_n_bound, 0, sizeof(int) * h->n_inst, h->stream);
     cudaMemsetAsync(h->d_sample_cursor, 0, sizeof(unsigned) * 4, h->stream);
@@ -2098,7 +2128,8 @@ int remc_energy_full(remc_handle* h, double* out) {
   int grid = std::min(h->n_items, h->num_sms * 8);
   energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
                                                    h->d_mol_start, h->d_items, h->n_items,
-                                                   h->d_scratch, h->d_scratch_cc, consts_of(h));
+                                                   h->d_scratch, h->d_scratch_cc, consts_of(h),
+                                                   h->d_err);
   REMC_CUDA_TRY(cudaGetLastError());
   energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(
       h->d_item_off, h->n_inst, h->d_scratch, h->d_scratch_cc, h->d_energy, h->d_ecc);
@@ -2106,7 +2137,7 @@ int remc_energy_full(remc_handle* h, double* out) {
   if (out) {
     REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_energy, sizeof(double) * h->n_inst,
                                   cudaMemcpyDeviceToHost, h->stream));
-    REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return check_device_error(h);
   }
   return REMC_OK;
 }
@@ -2115,8 +2146,7 @@ int remc_get_energies(remc_handle* h, double* out) {
   if (!h || !out) return set_error(REMC_ERR_INVALID, "null argument");
   REMC_CUDA_TRY(cudaMemcpyAsync(out, h->d_energy, sizeof(double) * h->n_inst,
                                 cudaMemcpyDeviceToHost, h->stream));
-  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return REMC_OK;
+  return check_device_error(h);
 }
 
 int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
@@ -2625,7 +2655,7 @@ int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* clust
 int remc_sync(remc_handle* h) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return REMC_OK;
+  return check_device_error(h);
 }
 
 int remc_num_instances(const remc_handle* h) { return h ? h->n_inst : 0; }
