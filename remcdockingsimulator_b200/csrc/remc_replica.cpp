@@ -589,6 +589,15 @@ void ReplicaExchange::download() {
   }
 }
 
+void ReplicaExchange::autotune(int probe_steps) {
+  check(remc_autotune(h_, probe_steps, seed_ ^ 0x5eedull, nullptr, nullptr, nullptr),
+        "remc_autotune");
+}
+
+void ReplicaExchange::setCluster(int ctas_per_replica) {
+  check(remc_set_cluster(h_, ctas_per_replica), "remc_set_cluster");
+}
+
 void ReplicaExchange::run(int n_blocks, int steps_per_block) {
   if (n_blocks <= 0) return;
   check(remc_run(h_, n_blocks, steps_per_block, seed_, step_, round_), "remc_run");

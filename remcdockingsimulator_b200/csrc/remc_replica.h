@@ -229,8 +229,13 @@ class ReplicaExchange {
   ReplicaExchange(const ReplicaExchange&) = delete;
   ReplicaExchange& operator=(const ReplicaExchange&) = delete;
   void run(int n_blocks, int steps_per_block);
-  // exchange rounds run so far, and their accepted swaps
+  // exchange rounds run so far
   int rounds() const { return round_; }
+  // Pick threads per replica, shared-memory layout and CTAs per replica by
+  // probe sweeps on these replicas (remc_autotune; the state is restored);
+  // or set the CTAs per replica directly (1, 2, 4 or 8).
+  void autotune(int probe_steps = 256);
+  void setCluster(int ctas_per_replica);
 
  private:
   void upload();

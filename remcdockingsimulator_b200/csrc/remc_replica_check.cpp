@@ -133,6 +133,8 @@ int remc_cmd(int argc, char** argv) {
   std::vector<Replica*> ptr;
   for (Replica& r : reps) ptr.push_back(&r);
   ReplicaExchange ex(ptr, seed);
+  // REMC_CHECK_CLUSTER=c runs the replicas on clusters of c CTAs
+  if (const char* c = std::getenv("REMC_CHECK_CLUSTER")) ex.setCluster(std::atoi(c));
   ex.run(blocks, steps);
   for (Replica* r : ptr) std::printf("%d %.9g %.17g\n", (int)r->label, r->temperature, r->potential);
   write_state(argv[11], ptr);

@@ -102,18 +102,23 @@ def test_facade_mcsearch_matches_engine_sweep(placed, tmp_path):
     assert sum(got["cnt"]) == steps
 
 
-def test_facade_replica_exchange_matches_engine_run(placed, tmp_path):
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_facade_replica_exchange_matches_engine_run(placed, tmp_path, cluster, monkeypatch):
     from remcdockingsimulator_b200.engine import Engine
     aa, pp, args, s = placed
     R, blocks, steps, seed = 6, 3, 200, 424242
     tmin, tmax = 290.0, 480.0
     outf = str(tmp_path / "remc.txt")
+    if cluster > 1:
+        monkeypatch.setenv("REMC_CHECK_CLUSTER", str(cluster))
     _check("remc", aa, pp, s.box, R, tmin, tmax, blocks, steps, seed, outf, *args)
     got = _read_state(outf)
     lad = geometric_ladder(tmin, tmax, R)
     with Engine([s], R) as eng:
         eng.set_replica_params([lad], np.full(R, np.float32(0.5), np.float32),
                                np.full(R, float(np.float32(0.2))))
+        if cluster > 1:
+            eng.set_cluster(cluster)
         eng.energy_full()
         eng.run(blocks, steps, seed, 0, 0)
         pos, rel, cen, quat = eng.download_state()
