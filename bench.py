@@ -421,9 +421,20 @@ def cpu_baseline(workload, seed: int):
         reps = build_reference_replicas(workload, systems)
         wall = time_reference(reps, cores, mc)
         n_rs = len(reps) * mc
+        # the reference's own Replica::E() on one core (its "Host Timer" figure,
+        # Replica.cpp:1082): inter-molecular pairs evaluated per second
+        r0 = reps[0]
+        s0 = workload.systems[systems[0]]
+        pairs = (s0.n_beads * (s0.n_beads - 1) - sum(m.n * (m.n - 1) for m in s0.molecules)) // 2
+        calls, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 1.0:
+            r0.E()
+            calls += 1
+        e_rate = pairs * calls / (time.perf_counter() - t0)
         for r in reps:
             r.close()
         return {"value": n_rs / wall, "unit": "replica-steps/s", "cores": min(cores, len(reps)),
+                "e_pairs_per_s_one_core": e_rate,
                 "kind": "reference",
                 "sample": "reference Replica::MCSearch (compiled from its sources, full energy "
                           "every step, its own (6/r)^6 crowder model and lambda=0.159) on all "
