@@ -26,6 +26,7 @@
 //                      parallel lanes (main.cpp:1427-1453).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -1462,6 +1463,14 @@ EnergyConsts consts_of(const remc_handle* h) {
   return K;
 }
 
+// NVTX range over one API call, for timelines (a no-op unless a tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // Report (and clear) the error word a kernel sets when a bounded wait gives up.
 int check_device_error(remc_handle* h) {
   int e = 0;
@@ -2011,6 +2020,7 @@ int remc_set_type_tables(remc_handle* h, const float* vdw, const float* charge, 
 
 int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const float* centre,
                       const double* quat) {
+  NvtxRange nvtx_range("remc_upload_state");
   if (!h || !pos || !rel || !centre || !quat) return set_error(REMC_ERR_INVALID, "null argument");
   const size_t nb = h->total_beads, nm = h->total_mols;
   float* sp = h->d_stage;
@@ -2064,6 +2074,7 @@ int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const 
 }
 
 int remc_download_state(remc_handle* h, float* pos, float* rel, float* centre, double* quat) {
+  NvtxRange nvtx_range("remc_download_state");
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->state_set) return set_error(REMC_ERR_STATE, "state not uploaded");
   const size_t nb = h->total_beads, nm = h->total_mols;
@@ -2123,6 +2134,7 @@ int remc_set_replica_params(remc_handle* h, const float* ladder, const float* ts
 }
 
 int remc_energy_full(remc_handle* h, double* out) {
+  NvtxRange nvtx_range("remc_energy_full");
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   int grid = std::min(h->n_items, h->num_sms * 8);
@@ -2150,6 +2162,7 @@ int remc_get_energies(remc_handle* h, double* out) {
 }
 
 int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
+  NvtxRange nvtx_range("remc_sweep");
   int rc = check_ready(h);
   if (rc) return rc;
   if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
@@ -2166,6 +2179,7 @@ int remc_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
 }
 
 int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0) {
+  NvtxRange nvtx_range("remc_sweep_plain");
   int rc = check_ready(h);
   if (rc) return rc;
   if (n_steps < 0) return set_error(REMC_ERR_INVALID, "n_steps < 0");
@@ -2191,6 +2205,7 @@ int remc_sweep_plain(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0)
 }
 
 int remc_exchange(remc_handle* h, uint64_t seed, uint32_t round, int offset) {
+  NvtxRange nvtx_range("remc_exchange");
   int rc = check_ready(h);
   if (rc) return rc;
   if (offset != 0 && offset != 1) return set_error(REMC_ERR_INVALID, "offset must be 0 or 1");
@@ -2364,6 +2379,7 @@ int remc_read_samples(remc_handle* h, remc_sample* records, int max_records,
 
 int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
                         double* dE_dlambda, double* dE_dxi, double* dE_deps, double* energy) {
+  NvtxRange nvtx_range("remc_energy_adjoint");
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   int rc = REMC_OK;
@@ -2498,6 +2514,7 @@ int remc_delta_energy(remc_handle* h, int inst, int mol, const float* new_pos, d
 
 int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, uint32_t step0,
              uint32_t round0) {
+  NvtxRange nvtx_range("remc_run");
   int rc = check_ready(h);
   if (rc) return rc;
   if (n_blocks < 0 || steps_per_block <= 0)
@@ -2543,6 +2560,7 @@ int remc_run(remc_handle* h, int n_blocks, int steps_per_block, uint64_t seed, u
 
 int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_out,
                   int* mol_in_smem_out, float* best_ms_out) {
+  NvtxRange nvtx_range("remc_autotune");
   int rc = check_ready(h);
   if (rc) return rc;
   if (probe_steps <= 0) return set_error(REMC_ERR_INVALID, "probe_steps must be positive");
