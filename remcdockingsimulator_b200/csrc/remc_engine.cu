@@ -235,7 +235,7 @@ struct SweepSmem {
     s.beads = take(off, sizeof(float4) * nmax);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
-    s.trial_rel = take(off, sizeof(float4) * lmax);
+    s.trial_rel = take(off, sizeof(float4) * 2 * lmax);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
@@ -281,7 +281,10 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   // rotated relative positions of the chain's beads, computed with its trial
   // positions by the beads' owners and installed by the same threads: the
   // install writes rel without reading it, so the CTAs of a cluster, which
-  // all install the same values, cannot read one another's update
+  // all install the same values, cannot read one another's update. Two
+  // buffers by step parity, like the trial positions: the next step's owners
+  // (another molecule, other threads) write theirs before any barrier, while
+  // slower warps may still install from this step's
   float4* s_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
   StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
@@ -366,9 +369,12 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   float p_nc0 = 0.f, p_nc1 = 0.f, p_nc2 = 0.f;          // accepted new centre
 
   for (int s = 0; s < n_steps; ++s) {
-    // ---- prefetch the next ring half (records s+32 .. s+63)
-    if ((s & 31) == 0 && s > 0 && s + 32 < n_steps) {
-      const int first = s + 32;
+    // ---- prefetch the next ring half (records s+31 .. s+62). The half it
+    // overwrites ends with step s-2's record, which is read until after step
+    // s-2's barrier; a thread at step s has passed step s-1's barrier, so no
+    // thread reads it any more
+    if ((s & 31) == 1 && s > 1 && s + 31 < n_steps) {
+      const int first = s + 31;
       const int nrec = min(32, n_steps - first);
       const int chunks = nrec * (int)(sizeof(StepRec) / 16);
       char* dst = reinterpret_cast<char*>(s_ring + (first & (kRing - 1)));
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         if (rec.rotate) {
           const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
           np = make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
-          s_trel[k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
+          s_trel[b * A.lmax + k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
         } else {
           np = make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
         }
@@ -450,12 +456,41 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         // one bead (a crowder or a one-residue chain), positions in registers
         const int ta = bead_type(pold1.w);
         const float4* trow = s_tab + ta * kNT;
-        for (int part = 0; part < 2; ++part) {
-          const int lo = part ? x1 : 0, hi = part ? N : x0;
-          if (lo >= hi) continue;
-          const int cb = min(hi, ncb);
-          int j = lo + ((gtid - lo) & gmask);  // first j >= lo in this thread's class
-          if (!rec.crowd) {
+        if (rec.crowd) {
+          // a one-bead crowder: every pair is a crowder pair. One loop over
+          // the thread's j in increasing order (the order of the per-thread
+          // sum), two j per pass with both loads issued first, the moved
+          // bead itself (j = m0) left out of the sum
+          const bool one_ct = ctype >= 0;
+          const float4 Tc = trow[one_ct ? ctype : 0];
+          int j = gtid;
+          for (; j + gstride < N; j += 2 * gstride) {
+            const int j2 = j + gstride;
+            const float4 pa = s_beads[j], pb = s_beads[j2];
+            const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
+            const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trow[bead_type(pb.w)];
+            const float ena = crowd_energy<R12, CUT>(pair_r2(pnew1, pa, box, invbox), Ta.x, Ta.z);
+            const float eoa = crowd_energy<R12, CUT>(pair_r2(pold1, pa, box, invbox), Ta.x, Ta.z);
+            const float enb = crowd_energy<R12, CUT>(pair_r2(pnew1, pb, box, invbox), Tb.x, Tb.z);
+            const float eob = crowd_energy<R12, CUT>(pair_r2(pold1, pb, box, invbox), Tb.x, Tb.z);
+            if (j != m0) acc_o += ena - eoa;
+            if (j2 != m0) acc_o += enb - eob;
+          }
+          if (j < N && j != m0) {
+            const float4 pa = s_beads[j];
+            const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
+            const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pa, box, invbox), Ta.x, Ta.z);
+            const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pa, box, invbox), Ta.x, Ta.z);
+            acc_o += en - eo;
+          }
+        } else {
+          // a one-residue chain: residue pairs with the chains' beads,
+          // crowder pairs with the rest
+          for (int part = 0; part < 2; ++part) {
+            const int lo = part ? x1 : 0, hi = part ? N : x0;
+            if (lo >= hi) continue;
+            const int cb = min(hi, ncb);
+            int j = lo + ((gtid - lo) & gmask);  // first j >= lo in this thread's class
             for (; j < cb; j += gstride) {
               const float4 pj = s_beads[j];
               const float4 Tj = trow[bead_type(pj.w)];
@@ -463,22 +498,14 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               const float eo = pair_energy_r2(pair_r2(pold1, pj, box, invbox), Tj, false, A.K);
               acc_c += en - eo;
             }
-          } else {
-            for (; j < cb; j += gstride) {
+            const float4 Tc = trow[ctype >= 0 ? ctype : 0];
+            for (; j < hi; j += gstride) {
               const float4 pj = s_beads[j];
-              const float4 Tj = trow[bead_type(pj.w)];
+              const float4 Tj = ctype >= 0 ? Tc : trow[bead_type(pj.w)];
               const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
               const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pj, box, invbox), Tj.x, Tj.z);
               acc_o += en - eo;
             }
-          }
-          const float4 Tc = trow[ctype >= 0 ? ctype : 0];
-          for (; j < hi; j += gstride) {
-            const float4 pj = s_beads[j];
-            const float4 Tj = ctype >= 0 ? Tc : trow[bead_type(pj.w)];
-            const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pj, box, invbox), Tj.x, Tj.z);
-            const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pj, box, invbox), Tj.x, Tj.z);
-            acc_o += en - eo;
           }
         }
       } else {
@@ -583,7 +610,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         int j = m0 + ((tid - m0) & tmask);
         for (; j < m0 + n; j += nthr) {
           s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
-          if (rec.rotate) A.rel[bead_off + j] = s_trel[j - m0];
+          if (rec.rotate) A.rel[bead_off + j] = s_trel[b * A.lmax + (j - m0)];
         }
       }
       if (tid == 0) {
