@@ -243,13 +243,13 @@ struct SweepSmem {
   }
 };
 
-// Sum of nw <= 8 FP64 partials in a fixed pairwise order (missing entries add
-// an exact zero); every thread evaluates it and gets the same value.
-__device__ __forceinline__ double tree_sum8(const double* v, int nw) {
-  double a[8];
-#pragma unroll
-  for (int w = 0; w < 8; ++w) a[w] = w < nw ? v[w] : 0.0;
-  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+// Sum of 8 FP64 partials (16-byte aligned) in a fixed pairwise order; the
+// entries of warps a smaller CTA does not have hold an exact zero. Every
+// thread evaluates it and gets the same value.
+__device__ __forceinline__ double tree_sum8(const double* v) {
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  const double2 a = v2[0], b = v2[1], c = v2[2], d = v2[3];
+  return ((a.x + a.y) + (b.x + b.y)) + ((c.x + c.y) + (d.x + d.y));
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
@@ -328,6 +328,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
+  // partial-sum entries of warps this CTA does not have: an exact zero
+  for (int i = tid; i < 2 * csize * 2 * 8; i += nthr)
+    if ((i & 7) >= nwarps) s_red[(i >> 3) * 32 + (i & 7)] = 0.0;
   for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
   // molecule centres: shared memory, or global memory for the largest
   // systems (thread 0 writes a centre; others read it only after a later
@@ -510,7 +513,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         }
       } else {
         // a chain (or a multi-bead crowder): each thread takes its beads j and
-        // runs over the n moved beads k, the same k in every lane
+        // runs over the n moved beads k, the same k in every lane. Two j per
+        // pass where the class has them, so each k's positions and table row
+        // serve two beads; each j's sum over k is added on its own, in j order
         const float4* oldp = same ? s_tpos + p_b * A.lmax : s_beads + m0;
         const float4* newp = s_tpos + b * A.lmax;
         for (int part = 0; part < 2; ++part) {
@@ -518,6 +523,26 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           if (lo >= hi) continue;
           const int cb = min(hi, ncb);
           int j = lo + ((gtid - lo) & gmask);
+          if (!rec.crowd) {
+            for (; j + gstride < cb; j += 2 * gstride) {
+              const float4 pa = s_beads[j], pb = s_beads[j + gstride];
+              const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+              float a = 0.0f, c = 0.0f;
+              for (int k = 0; k < n; ++k) {
+                const float4 po = oldp[k], pn = newp[k];
+                const float4* row = s_tab + bead_type(po.w) * kNT;
+                const float4 Ta = row[ta], Tb = row[tb];
+                const float ena = pair_energy_r2(pair_r2(pn, pa, box, invbox), Ta, false, A.K);
+                const float eoa = pair_energy_r2(pair_r2(po, pa, box, invbox), Ta, false, A.K);
+                const float enb = pair_energy_r2(pair_r2(pn, pb, box, invbox), Tb, false, A.K);
+                const float eob = pair_energy_r2(pair_r2(po, pb, box, invbox), Tb, false, A.K);
+                a += ena - eoa;
+                c += enb - eob;
+              }
+              acc_c += a;
+              acc_c += c;
+            }
+          }
           for (; j < cb; j += gstride) {
             const float4 pj = s_beads[j];
             const int tb = bead_type(pj.w);
@@ -541,6 +566,26 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               }
               acc_o += a;
             }
+          }
+          const bool one_ct = ctype >= 0;
+          for (; j + gstride < hi; j += 2 * gstride) {
+            const float4 pa = s_beads[j], pb = s_beads[j + gstride];
+            const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+            float a = 0.0f, c = 0.0f;
+            for (int k = 0; k < n; ++k) {
+              const float4 po = oldp[k], pn = newp[k];
+              const float4* row = s_tab + bead_type(po.w) * kNT;
+              const float4 Ta = row[ta];
+              const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
+              const float ena = crowd_energy<R12, CUT>(pair_r2(pn, pa, box, invbox), Ta.x, Ta.z);
+              const float eoa = crowd_energy<R12, CUT>(pair_r2(po, pa, box, invbox), Ta.x, Ta.z);
+              const float enb = crowd_energy<R12, CUT>(pair_r2(pn, pb, box, invbox), Tb.x, Tb.z);
+              const float eob = crowd_energy<R12, CUT>(pair_r2(po, pb, box, invbox), Tb.x, Tb.z);
+              a += ena - eoa;
+              c += enb - eob;
+            }
+            acc_o += a;
+            acc_o += c;
           }
           for (; j < hi; j += gstride) {
             const float4 pj = s_beads[j];
@@ -590,12 +635,12 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       // from registers instead (same && !p_rot)
       next_c = cent[s_ring[(s + 1) & (kRing - 1)].m];
     }
-    double dE = tree_sum8(s_red + b * csize * 64, nwarps);
+    double dE = tree_sum8(s_red + b * csize * 64);
     double dE_cc = 0.0;
-    if (!rec.crowd) dE_cc = tree_sum8(s_red + b * csize * 64 + 32, nwarps);
+    if (!rec.crowd) dE_cc = tree_sum8(s_red + b * csize * 64 + 32);
     for (int r = 1; r < csize; ++r) {  // the other CTAs' sums, in rank order
-      dE += tree_sum8(s_red + (b * csize + r) * 64, nwarps);
-      if (!rec.crowd) dE_cc += tree_sum8(s_red + (b * csize + r) * 64 + 32, nwarps);
+      dE += tree_sum8(s_red + (b * csize + r) * 64);
+      if (!rec.crowd) dE_cc += tree_sum8(s_red + (b * csize + r) * 64 + 32);
     }
     if (!rec.crowd) dE += dE_cc;
     const int acc = dE < 0.0 ? 1 : (dE < recs_.thr ? 2 : 0);
