@@ -106,18 +106,17 @@ struct EnergyConsts {
   int crowder_cut;   // 1: crowder pairs beyond the cutoff contribute nothing
 };
 
-// Round to nearest, ties to even, on the FMA pipe: adding and subtracting
-// 1.5 * 2^23 leaves the integer part of any |x| < 2^22 in the mantissa and
-// rounds exactly as rintf does (the rounding is the IEEE add's own).
-__device__ __forceinline__ float rint_fma_pipe(float x) {
-  const float kMagic = 12582912.0f;  // 1.5 * 2^23
-  return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
-}
-
-// Minimum image d - L*rint(d/L) per axis (CudaFunctions.cu:430-442 uses rintf);
-// |d/L| stays far below 2^22 for coordinates within a few box lengths.
+// Minimum image d - L*rint(d/L) per axis (CudaFunctions.cu:430-442 uses
+// rintf), on the FMA pipe: the FMA adds 1.5 * 2^23 to the exact product
+// d * (1/L) and rounds once, which leaves rint of that product (ties to even)
+// as the integer part of the sum for any |d/L| < 2^22; subtracting the
+// constant is exact. Rounding the product first and then adding would round
+// twice, and differ only where the product lies within half an ulp of a
+// half-integer, where both images are half a box away.
 __device__ __forceinline__ float min_image(float d, float L, float invL) {
-  return fmaf(-L, rint_fma_pipe(d * invL), d);
+  const float kMagic = 12582912.0f;  // 1.5 * 2^23
+  const float n = __fsub_rn(__fmaf_rn(d, invL, kMagic), kMagic);
+  return fmaf(-L, n, d);
 }
 
 // Energy (kcal/mol) of one pair of beads of different molecules at squared

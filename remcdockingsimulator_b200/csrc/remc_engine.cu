@@ -1115,8 +1115,89 @@ __device__ __forceinline__ void adjoint_group(
   }
 }
 
+// The common case of adjoint_group: crowder beads j of one species (fixed
+// table entry Tc) and a group that needs no per-pair tests, evaluated two
+// pairs at a time in packed FP32 (f32x2: one instruction per operation on
+// both pairs, each element rounded as the scalar operation would be). The
+// lane pairs its beads q and q + 4 (j = jg + (q ^ r) and jg + ((q + 4) ^ r)),
+// exactly the two the first transpose-reduce level combines, so the j forces
+// land in the same registers as in adjoint_group. Coordinates come from the
+// tile's structure-of-arrays copy, so both beads' x (y, z) load straight into
+// one register pair. Works with e = p_j - p_i = -d: the forces it sums are
+// the negated pair forces (the caller negates the i-force sums; the j beads
+// receive them as they are).
 template <bool R12, bool CUT>
-__global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
+__device__ __forceinline__ void adjoint_group_crowd2(
+    const float* __restrict__ s_jx, const float* __restrict__ s_jy,
+    const float* __restrict__ s_jz, float (*__restrict__ s_fjw)[3], int jg, int jend,
+    float2 npx, float2 npy, float2 npz, float A, float cut2, float box, float invbox, int lane,
+    float2& nfx, float2& nfy, float2& nfz, float2& acc_e2) {
+  const int r = (lane >> 2) & 7;
+  const float kMagic = 12582912.0f;  // 1.5 * 2^23, as in min_image
+  const float2 iL = make_float2(invbox, invbox), nL = make_float2(-box, -box);
+  const float2 M = make_float2(kMagic, kMagic), nM = make_float2(-kMagic, -kMagic);
+  const float2 A2 = make_float2(A, A);
+  const float2 cf = make_float2(R12 ? 12.0f : 6.0f, R12 ? 12.0f : 6.0f);
+  float g[8][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int ja = jg + (q ^ r), jb = jg + ((q + 4) ^ r);
+    float2 ex = __fadd2_rn(make_float2(s_jx[ja], s_jx[jb]), npx);
+    float2 ey = __fadd2_rn(make_float2(s_jy[ja], s_jy[jb]), npy);
+    float2 ez = __fadd2_rn(make_float2(s_jz[ja], s_jz[jb]), npz);
+    ex = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ex, iL, M), nM), ex);
+    ey = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ey, iL, M), nM), ey);
+    ez = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ez, iL, M), nM), ez);
+    const float2 r2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
+    const float2 rinv = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
+    const float2 rinv2 = __fmul2_rn(rinv, rinv);
+    const float2 i6 = __fmul2_rn(__fmul2_rn(rinv2, rinv2), rinv2);
+    float2 e = __fmul2_rn(A2, i6);
+    if (R12) e = __fmul2_rn(e, i6);
+    if (CUT) {
+      e.x = (r2.x < cut2) ? e.x : 0.0f;
+      e.y = (r2.y < cut2) ? e.y : 0.0f;
+    }
+    acc_e2 = __fadd2_rn(acc_e2, e);
+    const float2 f = __fmul2_rn(__fmul2_rn(cf, e), rinv2);  // -(de/dr)/r
+    const float2 gx = __fmul2_rn(f, ex), gy = __fmul2_rn(f, ey), gz = __fmul2_rn(f, ez);
+    nfx = __fadd2_rn(nfx, gx);
+    nfy = __fadd2_rn(nfy, gy);
+    nfz = __fadd2_rn(nfz, gz);
+    g[q][0] = gx.x;
+    g[q][1] = gy.x;
+    g[q][2] = gz.x;
+    g[q + 4][0] = gx.y;
+    g[q + 4][1] = gy.y;
+    g[q + 4][2] = gz.y;
+  }
+  float h4[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h4[q][c] = g[q][c] + __shfl_xor_sync(0xffffffffu, g[q + 4][c], 16);
+  float h2[2][3];
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h2[q][c] = h4[q][c] + __shfl_xor_sync(0xffffffffu, h4[q + 2][c], 8);
+  float h1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h1[c] = h2[0][c] + __shfl_xor_sync(0xffffffffu, h2[1][c], 4);
+    h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 2);
+    h1[c] += __shfl_xor_sync(0xffffffffu, h1[c], 1);
+  }
+  if ((lane & 3) == 0 && jg + r < jend) {
+    // force on j = sum over this warp's i beads of the negated pair forces
+    s_fjw[jg + r][0] += h1[0];
+    s_fjw[jg + r][1] += h1[1];
+    s_fjw[jg + r][2] += h1[2];
+  }
+}
+
+template <bool R12, bool CUT>
+__global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
     const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
@@ -1124,6 +1205,7 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     double* __restrict__ e_out, EnergyConsts K, AdjConsts C) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
+  __shared__ float s_jx[kTile], s_jy[kTile], s_jz[kTile];  // the j tile again, by coordinate
   __shared__ float s_fj[kTile / 32][kTile][3];
   __shared__ float s_G[kNumAmino * kNumAmino];
   __shared__ double s_red[kTile / 32][2];
@@ -1138,7 +1220,13 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
     __syncthreads();  // the previous item is done with the shared buffers
-    if (tid < jn) s_j[tid] = pos[base + j0 + tid];
+    if (tid < jn) {
+      const float4 p = pos[base + j0 + tid];
+      s_j[tid] = p;
+      s_jx[tid] = p.x;
+      s_jy[tid] = p.y;
+      s_jz[tid] = p.z;
+    }
     for (int k = tid; k < (kTile / 32) * kTile * 3; k += kTile) (&s_fj[0][0][0])[k] = 0.0f;
     for (int k = tid; k < kNumAmino * kNumAmino; k += kTile) s_G[k] = 0.0f;
     __syncthreads();
@@ -1159,6 +1247,10 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
     const bool tc_fixed = S.crowd_type >= 0;
     const float4 Tc = s_tab[(tc_fixed ? S.crowd_type : 0) * kNT + ta];
     float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
+    // packed crowder groups: negated force sums and energy, two pairs per lane
+    float2 nfx = make_float2(0.f, 0.f), nfy = nfx, nfz = nfx, acc_e2 = nfx;
+    const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+                 npz = make_float2(-pi.z, -pi.z);
     // a group needs no per-pair tests when, for every lane, it is full, past
     // the lane's first j and clear of its own molecule (a warp vote)
 #define REMC_ADJ_GROUP(CHAIN_, jend_)                                                           \
@@ -1174,8 +1266,25 @@ __global__ void __launch_bounds__(kTile) adjoint_tile_kernel(
                                             invbox, K, C, lane, fx, fy, fz, acc_e, acc_x);    \
   }
     for (int jg = 0; jg < jc; jg += 8) REMC_ADJ_GROUP(true, jc)  // uniform trip counts
-    for (int jg = jc; jg < jn; jg += 8) REMC_ADJ_GROUP(false, jn)
+    if (tc_fixed) {
+      for (int jg = jc; jg < jn; jg += 8) {
+        const bool clean = ivalid && jg + 8 <= jn && jg >= jlo && (ex1 <= jg || ex0 >= jg + 8);
+        if (__all_sync(0xffffffffu, clean))
+          adjoint_group_crowd2<R12, CUT>(s_jx, s_jy, s_jz, s_fj[warp], jg, jn, npx, npy, npz,
+                                         Tc.x, Tc.z, box, invbox, lane, nfx, nfy, nfz, acc_e2);
+        else
+          adjoint_group<R12, CUT, false, true>(s_j, s_tab, s_G, s_fj[warp], jg, jn, jlo, ex0, ex1,
+                                               ivalid, pi, ta, a_crowd, Tc, tc_fixed, box, invbox,
+                                               K, C, lane, fx, fy, fz, acc_e, acc_x);
+      }
+    } else {
+      for (int jg = jc; jg < jn; jg += 8) REMC_ADJ_GROUP(false, jn)
+    }
 #undef REMC_ADJ_GROUP
+    fx -= nfx.x + nfx.y;
+    fy -= nfy.x + nfy.y;
+    fz -= nfz.x + nfz.y;
+    acc_e += acc_e2.x + acc_e2.y;
     double de = warp_sum((double)acc_e), dxv = warp_sum((double)acc_x);
     if (lane == 0) {
       s_red[warp][0] = de;

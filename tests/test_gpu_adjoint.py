@@ -56,6 +56,11 @@ def test_adjoint_crowded_r12(built_lib):
     _check("crowded", 21)
 
 
+def test_adjoint_crowded_reference_crowders(built_lib):
+    """The reference's crowder model: (6/r)^6 walls cut at 15 A."""
+    _check("crowded", 23, mode_ref=True)
+
+
 def test_adjoint_two_chain(built_lib):
     _check("two_chain", 22)
 
