@@ -56,11 +56,13 @@ class Engine:
                     np.array_equal(s.table.charge, table0.charge) and
                     np.array_equal(s.table.pairs, table0.pairs)):
                 raise ValueError("all systems of one engine must share the residue tables")
-        # crowder species: one type per distinct crowder radius
+        # crowder species: one type per distinct crowder radius over all
+        # systems (a system's own species numbering is mapped onto these)
         radii: List[float] = []
         for s in self.systems:
-            if any(m.crowder for m in s.molecules) and s.crowder_radius not in radii:
-                radii.append(s.crowder_radius)
+            for r in s.crowder_radii():
+                if r not in radii:
+                    radii.append(r)
         if len(radii) > MAX_TYPES - NUM_AMINO:
             raise ValueError("at most %d distinct crowder radii" % (MAX_TYPES - NUM_AMINO))
         self._species = {r: NUM_AMINO + i for i, r in enumerate(radii)}
@@ -68,9 +70,12 @@ class Engine:
         descs = (SystemDesc * len(self.systems))()
         for i, s in enumerate(self.systems):
             mol_start, roles, types = s.topology()
-            if s.crowder_radius in self._species:
-                types = types.copy()
-                types[types >= NUM_AMINO] = self._species[s.crowder_radius]
+            local = s.crowder_radii()
+            if local:
+                remap = np.arange(MAX_TYPES, dtype=np.int32)
+                for k, r in enumerate(local):
+                    remap[NUM_AMINO + k] = self._species[r]
+                types = remap[types]
             self._topo.append((mol_start, roles, types))
             d = descs[i]
             d.n_beads = s.n_beads

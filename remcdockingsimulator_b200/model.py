@@ -226,6 +226,7 @@ class Molecule:
     crowder: bool = False
     name: str = ""
     res_seq: Optional[np.ndarray] = None  # PDB residue numbers (Residue::resSeq)
+    radius: Optional[float] = None  # a crowder's own radius (else the system's)
 
     @property
     def n(self) -> int:
@@ -259,7 +260,7 @@ class Molecule:
     def copy(self) -> "Molecule":
         return Molecule(self.types.copy(), self.pos.copy(), self.rel.copy(), self.centre.copy(),
                         self.quat.copy(), self.crowder, self.name,
-                        None if self.res_seq is None else self.res_seq.copy())
+                        None if self.res_seq is None else self.res_seq.copy(), self.radius)
 
     def translate(self, v) -> None:
         """Molecule::translate: centre and every bead += v (FP32)."""
@@ -399,14 +400,32 @@ class System:
     def n_chains(self) -> int:
         return sum(1 for m in self.molecules if not m.crowder)
 
+    def radius_of(self, m: Molecule) -> float:
+        return float(self.crowder_radius if m.radius is None else m.radius)
+
+    def crowder_radii(self) -> List[float]:
+        """Distinct crowder radii in order of first appearance; crowder
+        species k (bead type CROWDER_TYPE + k) has the k-th of them."""
+        radii: List[float] = []
+        for m in self.molecules:
+            if m.crowder and self.radius_of(m) not in radii:
+                radii.append(self.radius_of(m))
+        if len(radii) > MAX_TYPES - CROWDER_TYPE:
+            raise ModelError("at most %d crowder radii per system" % (MAX_TYPES - CROWDER_TYPE))
+        return radii
+
     def topology(self):
         mol_start = np.zeros(self.n_mol + 1, np.int32)
         roles = np.zeros(self.n_mol, np.int32)
         types = []
+        radii = self.crowder_radii()
         for i, m in enumerate(self.molecules):
             mol_start[i + 1] = mol_start[i] + m.n
             roles[i] = -1 if m.crowder else 0
-            types.append(np.full(m.n, CROWDER_TYPE, np.int32) if m.crowder else m.types)
+            if m.crowder:
+                types.append(np.full(m.n, CROWDER_TYPE + radii.index(self.radius_of(m)), np.int32))
+            else:
+                types.append(m.types)
         return mol_start, roles, np.concatenate(types).astype(np.int32)
 
     def state(self):
@@ -418,8 +437,8 @@ class System:
 
     def type_tables(self):
         """(vdw, charge, rho) per engine type: residue types from the table,
-        rho = vdW/2 for residues; crowder species 20.. carry the crowder
-        radius."""
+        rho = vdW/2 for residues; crowder species 20.. carry their crowder
+        radius (the system's radius where no species uses the type)."""
         vdw = np.zeros(MAX_TYPES, np.float32)
         q = np.zeros(MAX_TYPES, np.float32)
         rho = np.zeros(MAX_TYPES, np.float32)
@@ -427,6 +446,8 @@ class System:
         q[:20] = self.table.charge
         rho[:20] = self.table.vdw * np.float32(0.5)
         rho[20:] = np.float32(self.crowder_radius)
+        for k, r in enumerate(self.crowder_radii()):
+            rho[CROWDER_TYPE + k] = np.float32(r)
         return vdw, q, rho
 
 

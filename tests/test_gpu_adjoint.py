@@ -8,11 +8,11 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _check(name, seed, mode_ref=False):
+def _check(name, seed, mode_ref=False, w=None):
     from oracle import bindings as ob
     from remcdockingsimulator_b200 import synth
     from remcdockingsimulator_b200.engine import Engine, make_params
-    w = synth.WORKLOADS[name](seed)
+    w = synth.WORKLOADS[name](seed) if w is None else w
     s = w.systems[0]
     p = make_params(lambda_=0.16) if mode_ref else w.params
     R = 2

@@ -184,3 +184,27 @@ def test_oracle_translation_invariance(oracle_built, built_lib):
     e = o.energy(pos)
     shifted = (pos + np.float32(s.box)).astype(np.float32)  # one box image
     assert o.energy(shifted) == pytest.approx(e, rel=1e-5)
+
+
+def test_mixed_crowder_species_topology(oracle_built):
+    """Crowders with their own radii become species 20, 21, ... in order of
+    first appearance, carrying those radii in the type tables."""
+    from oracle import bindings as ob
+    from remcdockingsimulator_b200 import synth
+    w = synth.crowded(3)
+    s = w.systems[0]
+    radii = (12.0, 9.0, 7.0)
+    crowders = [m for m in s.molecules if m.crowder]
+    for k, m in enumerate(crowders):
+        m.radius = radii[k % 3]
+    assert s.crowder_radii() == list(radii)
+    _, _, types = s.topology()
+    ncb = sum(m.n for m in s.molecules if not m.crowder)
+    assert list(types[ncb:ncb + 6]) == [20, 21, 22, 20, 21, 22]
+    assert list(s.type_tables()[2][20:23]) == list(radii)
+    # in the r^-12 model the radii enter the energy
+    e_mixed = ob.FP64Oracle(s, w.params).energy(s.state()[0])
+    for m in crowders:
+        m.radius = None
+    e_one = ob.FP64Oracle(s, w.params).energy(s.state()[0])
+    assert abs(e_mixed - e_one) > 1e-3 * abs(e_one)
