@@ -224,6 +224,15 @@ int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem);
  * counterpart. */
 int remc_set_cluster(remc_handle* h, int cluster);
 int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* cluster);
+/* Where the sweep keeps each replica's beads: 1 = resident in shared memory
+ * (the default whenever the largest system fits), 0 = in place in global
+ * memory, with the chain's trial buffers in global scratch. Systems too large
+ * for shared memory (about 13,000 beads, or chains of thousands of residues)
+ * get 0 at remc_create; the reference's GPU path has no size limit either
+ * (CudaFunctions.cu:304-385 tiles over global memory). Results are identical
+ * either way. No reference counterpart. */
+int remc_set_bead_storage(remc_handle* h, int in_shared_memory);
+int remc_get_bead_storage(remc_handle* h, int* in_shared_memory);
 
 int remc_sync(remc_handle* h);
 int remc_num_instances(const remc_handle* h);

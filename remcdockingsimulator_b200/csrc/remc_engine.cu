@@ -211,6 +211,9 @@ struct SweepArgs {
   int nmax, mmax, lmax;  // shared-memory capacities
   int mol_in_smem;       // centres resident in shared memory
   int csize;             // CTAs per replica (a thread-block cluster), 1, 2, 4 or 8
+  // beads kept in global memory (systems too large for shared memory): trial
+  // positions and trial relative positions of each (instance, CTA rank), 4 lmax
+  float4* trial_scratch;
   EnergyConsts K;
 };
 
@@ -226,16 +229,17 @@ struct SweepSmem {
     return o;
   }
   // mol_in_smem = 0: molecule centres and starts stay in global memory (the
-  // largest systems), everything else as usual
+  // largest systems), everything else as usual. beads_in_smem = 0: the beads
+  // and the trial buffers stay in global memory too (systems of any size)
   static __host__ __device__ SweepSmem make(int nmax, int mmax, int lmax, int mol_in_smem,
-                                            int csize = 1) {
+                                            int csize = 1, int beads_in_smem = 1) {
     SweepSmem s;
     size_t off = 0;
     s.tab = take(off, sizeof(float4) * kNT * kNT);
-    s.beads = take(off, sizeof(float4) * nmax);
+    s.beads = take(off, beads_in_smem ? sizeof(float4) * nmax : 0);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
-    s.trial_pos = take(off, sizeof(float4) * 2 * lmax);
-    s.trial_rel = take(off, sizeof(float4) * 2 * lmax);
+    s.trial_pos = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
+    s.trial_rel = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
@@ -270,14 +274,20 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the trial buffer rather than from another thread's not-yet-ordered write.
 // A step of a one-bead molecule therefore costs one barrier; a chain step
 // costs two (trial positions are built by the owners of the chain's beads).
-template <bool R12, bool CUT, bool CLUSTER>
+// GB: the beads stay where they are in global memory (updated in place, no
+// prologue copy and no write-back) and the trial buffers live in per-instance
+// global scratch; every access pattern, owner and barrier is the same as with
+// the beads in shared memory (a CTA barrier orders global memory for the CTA,
+// a cluster barrier for the cluster; the CTAs of a cluster write identical
+// values to the beads they own).
+template <bool R12, bool CUT, bool CLUSTER, bool GB>
 __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem, A.csize);
+  const SweepSmem L = SweepSmem::make(A.nmax, A.mmax, A.lmax, A.mol_in_smem, A.csize, !GB);
   float4* s_tab = reinterpret_cast<float4*>(smem_raw + L.tab);
-  float4* s_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
+  float4* const sm_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
-  float4* s_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
+  float4* const sm_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
   // rotated relative positions of the chain's beads, computed with its trial
   // positions by the beads' owners and installed by the same threads: the
   // install writes rel without reading it, so the CTAs of a cluster, which
@@ -285,7 +295,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   // buffers by step parity, like the trial positions: the next step's owners
   // (another molecule, other threads) write theirs before any barrier, while
   // slower warps may still install from this step's
-  float4* s_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
+  float4* const sm_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
   StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
 
@@ -325,13 +335,18 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   const float box = S.box, invbox = S.invbox;
   const StepRec* recs = A.recs + (size_t)inst * A.rec_stride + A.rec_offset;
   const int n_steps = A.n_steps;
+  float4* const s_beads = GB ? A.pos + bead_off : sm_beads;
+  float4* const s_tpos =
+      GB ? A.trial_scratch + ((size_t)inst * csize + crank) * 4 * (size_t)A.lmax : sm_tpos;
+  float4* const s_trel = GB ? s_tpos + 2 * (size_t)A.lmax : sm_trel;
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
   // partial-sum entries of warps this CTA does not have: an exact zero
   for (int i = tid; i < 2 * csize * 2 * 8; i += nthr)
     if ((i & 7) >= nwarps) s_red[(i >> 3) * 32 + (i & 7)] = 0.0;
-  for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
+  if (!GB)
+    for (int i = tid; i < N; i += nthr) s_beads[i] = A.pos[bead_off + i];
   // molecule centres: shared memory, or global memory for the largest
   // systems (thread 0 writes a centre; others read it only after a later
   // barrier, which orders global memory within the CTA as well)
@@ -758,7 +773,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   // ---- epilogue: write the instance back (every CTA of a cluster holds the
   // same state; rank 0 writes it)
   if (crank == 0) {
-  for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
+  if (!GB)
+    for (int i = tid; i < N; i += nthr) A.pos[bead_off + i] = s_beads[i];
   if (A.mol_in_smem)
     for (int i = tid; i < M; i += nthr) A.centre[mol_off + i] = s_cent[i];
   }
@@ -1524,6 +1540,9 @@ struct remc_handle {
   int sweep_grid = 0;  // resident CTAs of the persistent sweep
   int mol_in_smem = 1; // molecule centres/starts in shared memory (else global)
   int sweep_csize = 1; // CTAs per replica (thread-block cluster size)
+  int beads_in_smem = 1; // beads resident in shared memory (else updated in place in global)
+  float4* d_trial_scratch = nullptr;  // trial buffers when the beads stay in global memory
+  size_t trial_scratch_cap = 0;       // float4 entries
   int max_dyn_smem = 0;
   int config_gen = 0;  // bumped when the sweep schedule changes
   TileItem* d_items = nullptr;
@@ -1588,7 +1607,7 @@ void free_all(remc_handle* h) {
                   h->d_dxi,        h->d_eadj,     h->d_mft,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad,
-                  h->d_err};
+                  h->d_err,      h->d_trial_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1689,33 +1708,37 @@ int ensure_recs(remc_handle* h, size_t steps) {
 }
 
 // The sweep kernel compiled for the handle's crowder model, single CTAs or
-// clusters of CTAs per replica.
+// clusters of CTAs per replica, beads in shared or in global memory.
 using SweepFn = void (*)(SweepArgs);
-SweepFn sweep_fn(const remc_params& p, bool cluster) {
+template <bool CLUSTER, bool GB>
+SweepFn sweep_fn_model(const remc_params& p) {
   const bool cut = p.crowder_cutoff > 0.0f;
-  if (cluster) {
-    if (p.crowder_mode) return cut ? sweep_kernel<true, true, true> : sweep_kernel<true, false, true>;
-    return cut ? sweep_kernel<false, true, true> : sweep_kernel<false, false, true>;
-  }
-  if (p.crowder_mode) return cut ? sweep_kernel<true, true, false> : sweep_kernel<true, false, false>;
-  return cut ? sweep_kernel<false, true, false> : sweep_kernel<false, false, false>;
+  if (p.crowder_mode)
+    return cut ? sweep_kernel<true, true, CLUSTER, GB> : sweep_kernel<true, false, CLUSTER, GB>;
+  return cut ? sweep_kernel<false, true, CLUSTER, GB> : sweep_kernel<false, false, CLUSTER, GB>;
+}
+SweepFn sweep_fn(const remc_params& p, bool cluster, bool global_beads) {
+  if (global_beads)
+    return cluster ? sweep_fn_model<true, true>(p) : sweep_fn_model<false, true>(p);
+  return cluster ? sweep_fn_model<true, false>(p) : sweep_fn_model<false, false>(p);
 }
 
-// Set the sweep schedule: threads per replica and where molecule data lives.
-int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize) {
+// Set the sweep schedule: threads per replica, where molecule data lives,
+// CTAs per replica, and whether the beads are resident in shared memory.
+int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize, int beads_in_smem) {
   if (threads < 32 || threads > 256 || (threads & (threads - 1)) != 0)
     return set_error(REMC_ERR_INVALID, "threads per replica must be 32, 64, 128 or 256");
   if (csize != 1 && csize != 2 && csize != 4 && csize != 8)
     return set_error(REMC_ERR_INVALID, "cluster size must be 1, 2, 4 or 8");
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem, csize).total;
+  const size_t smem =
+      SweepSmem::make(h->nmax, h->mmax, h->lmax, mol_in_smem, csize, beads_in_smem).total;
   if (smem > (size_t)h->max_dyn_smem)
     return set_error(REMC_ERR_INVALID,
                      "largest system needs %zu bytes of shared memory, device allows %d", smem,
                      h->max_dyn_smem);
+  const SweepFn fn = sweep_fn(h->params, csize > 1, !beads_in_smem);
   int per_sm = 0;
-  cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_fn(h->params, csize > 1), threads,
-                                                    smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
   if (e != cudaSuccess || per_sm < 1)
     return set_error(REMC_ERR_CUDA, "sweep kernel does not fit on an SM: %s",
                      cudaGetErrorString(e));
@@ -1733,14 +1756,29 @@ int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, sweep_fn(h->params, true), &cfg);
+    e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
     if (e != cudaSuccess || clusters < 1)
       return set_error(REMC_ERR_INVALID, "a cluster of %d sweep CTAs does not fit: %s", csize,
                        cudaGetErrorString(e));
   }
+  if (!beads_in_smem) {
+    // trial buffers of every (instance, CTA rank): 4 lmax float4 each
+    const size_t need = (size_t)h->n_inst * csize * 4 * (size_t)h->lmax;
+    if (need > h->trial_scratch_cap) {
+      float4* p = nullptr;
+      if (dev_alloc(&p, need)) return REMC_ERR_NOMEM;
+      if (h->d_trial_scratch) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->d_trial_scratch);
+      }
+      h->d_trial_scratch = p;
+      h->trial_scratch_cap = need;
+    }
+  }
   h->sweep_threads = threads;
   h->mol_in_smem = mol_in_smem;
   h->sweep_csize = csize;
+  h->beads_in_smem = beads_in_smem;
   h->sweep_grid = per_sm * h->num_sms;
   h->config_gen++;
   return REMC_OK;
@@ -1832,10 +1870,13 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   A.mmax = h->mmax;
   A.mol_in_smem = h->mol_in_smem;
   A.lmax = h->lmax;
+  A.trial_scratch = h->d_trial_scratch;
   A.K = consts_of(h);
-  const size_t smem = SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem, csize).total;
+  const bool gb = !h->beads_in_smem;
+  const size_t smem =
+      SweepSmem::make(h->nmax, h->mmax, h->lmax, h->mol_in_smem, csize, h->beads_in_smem).total;
   if (csize == 1) {
-    sweep_fn(h->params, false)<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
+    sweep_fn(h->params, false, gb)<<<n_blocks, h->sweep_threads, smem, h->stream>>>(A);
   } else {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -1849,7 +1890,7 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
     cfg.stream = h->stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    REMC_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_fn(h->params, true), A));
+    REMC_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_fn(h->params, true, gb), A));
   }
   REMC_CUDA_TRY(cudaGetLastError());
   return REMC_OK;
@@ -1998,11 +2039,15 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   int max_smem = 0;
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-  const SweepFn kSweeps[8] = {
-      sweep_kernel<false, false, false>, sweep_kernel<false, true, false>,
-      sweep_kernel<true, false, false>,  sweep_kernel<true, true, false>,
-      sweep_kernel<false, false, true>,  sweep_kernel<false, true, true>,
-      sweep_kernel<true, false, true>,   sweep_kernel<true, true, true>};
+  const SweepFn kSweeps[16] = {
+      sweep_kernel<false, false, false, false>, sweep_kernel<false, true, false, false>,
+      sweep_kernel<true, false, false, false>,  sweep_kernel<true, true, false, false>,
+      sweep_kernel<false, false, true, false>,  sweep_kernel<false, true, true, false>,
+      sweep_kernel<true, false, true, false>,   sweep_kernel<true, true, true, false>,
+      sweep_kernel<false, false, false, true>,  sweep_kernel<false, true, false, true>,
+      sweep_kernel<true, false, false, true>,   sweep_kernel<true, true, false, true>,
+      sweep_kernel<false, false, true, true>,   sweep_kernel<false, true, true, true>,
+      sweep_kernel<true, false, true, true>,    sweep_kernel<true, true, true, true>};
   int static_smem = 0;
   for (SweepFn f : kSweeps) {
     cudaFuncAttributes fattr;
@@ -2023,11 +2068,13 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     }
   }
   // default schedule (the autotuner may replace it): molecule data in shared
-  // memory when it fits, more threads per replica for larger systems
+  // memory when it fits, more threads per replica for larger systems, and the
+  // beads left in global memory for systems too large for shared memory
   {
     const int threads = h->nmax <= 2048 ? 128 : 256;
-    int rc0 = configure_sweep(h, threads, 1, 1);
-    if (rc0) rc0 = configure_sweep(h, threads, 0, 1);
+    int rc0 = configure_sweep(h, threads, 1, 1, 1);
+    if (rc0) rc0 = configure_sweep(h, threads, 0, 1, 1);
+    if (rc0) rc0 = configure_sweep(h, threads, 0, 1, 0);
     if (rc0) {
       delete h;
       return rc0;
@@ -2787,6 +2834,7 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   for (int c = 2; c <= 8; c *= 2)
     if ((long long)h->n_inst * c <= 2LL * h->num_sms) cand_c[n_c++] = c;
   int best_t = h->sweep_threads, best_m = h->mol_in_smem, best_c = h->sweep_csize;
+  int best_b = h->beads_in_smem;
   float best = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
@@ -2794,7 +2842,12 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   for (int ci = 0; ci < n_c && !rc; ++ci) {
   for (int ti = 0; ti < 2 && !rc; ++ti) {
     for (int mi = 1; mi >= 0 && !rc; --mi) {
-      if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci]) != REMC_OK) continue;
+      // beads in global memory only where they do not fit in shared memory
+      int bi = 1;
+      if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci], 1) != REMC_OK) {
+        if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci], 0) != REMC_OK) continue;
+        bi = 0;
+      }
       float ms = 0.0f;
       for (int rep = 0; rep < 2 && !rc; ++rep) {  // first launch warms up
         cudaEventRecord(e0, h->stream);
@@ -2813,6 +2866,7 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
         best_t = cand_threads[ti];
         best_m = mi;
         best_c = cand_c[ci];
+        best_b = bi;
       }
     }
   }
@@ -2823,7 +2877,7 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   cudaStreamSynchronize(h->stream);
   release();
   if (rc) return rc;
-  rc = configure_sweep(h, best_t, best_m, best_c);
+  rc = configure_sweep(h, best_t, best_m, best_c, best_b);
   if (rc) return rc;
   if (threads_out) *threads_out = best_t;
   if (mol_in_smem_out) *mol_in_smem_out = best_m;
@@ -2834,13 +2888,26 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
 int remc_set_schedule(remc_handle* h, int threads, int mol_in_smem) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return configure_sweep(h, threads, mol_in_smem ? 1 : 0, h->sweep_csize);
+  return configure_sweep(h, threads, mol_in_smem ? 1 : 0, h->sweep_csize, h->beads_in_smem);
 }
 
 int remc_set_cluster(remc_handle* h, int cluster) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return configure_sweep(h, h->sweep_threads, h->mol_in_smem, cluster);
+  return configure_sweep(h, h->sweep_threads, h->mol_in_smem, cluster, h->beads_in_smem);
+}
+
+int remc_set_bead_storage(remc_handle* h, int in_shared_memory) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return configure_sweep(h, h->sweep_threads, h->mol_in_smem, h->sweep_csize,
+                         in_shared_memory ? 1 : 0);
+}
+
+int remc_get_bead_storage(remc_handle* h, int* in_shared_memory) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (in_shared_memory) *in_shared_memory = h->beads_in_smem;
+  return REMC_OK;
 }
 
 int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* cluster) {

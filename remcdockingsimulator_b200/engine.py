@@ -353,6 +353,16 @@ class Engine:
     def set_schedule(self, threads: int, mol_in_smem: bool) -> None:
         check(lib().remc_set_schedule(self._h, threads, 1 if mol_in_smem else 0))
 
+    def set_bead_storage(self, shared: bool) -> None:
+        """Beads resident in shared memory (True) or updated in place in
+        global memory (False; any system size, same results)."""
+        check(lib().remc_set_bead_storage(self._h, 1 if shared else 0))
+
+    def beads_in_shared_memory(self) -> bool:
+        v = C.c_int()
+        check(lib().remc_get_bead_storage(self._h, C.byref(v)))
+        return bool(v.value)
+
     def stream_ptr(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         s = C.c_void_p(0)

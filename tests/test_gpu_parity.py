@@ -85,7 +85,8 @@ def test_delta_energy_api_vs_oracle(built_lib):
             assert abs(d_gpu - d_ref) <= E_RTOL * max(scale, 1e-3), (m, d_gpu, d_ref)
 
 
-def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None, cluster=1):
+def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None, cluster=1,
+                         beads_shared=True):
     from oracle import bindings as ob
     s = w.systems[0]
     lad = w.ladders[0][:R]
@@ -96,6 +97,9 @@ def _run_sweep_vs_oracle(w, R, n_steps, seed, step0=0, tsteps=None, rsteps=None,
         if cluster > 1:
             eng.set_cluster(cluster)
             assert eng.schedule()[2] == cluster
+        if not beads_shared:
+            eng.set_bead_storage(False)
+            assert not eng.beads_in_shared_memory()
         e0 = eng.energy_full()
         eng.sweep(n_steps, seed, step0)
         e_run = eng.energies()
