@@ -162,6 +162,46 @@ __device__ __forceinline__ float pair_r2(float4 a, float4 b, float L, float invL
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
+// ---------------------------------------------------------------- packed pairs
+// Two pairs per lane in packed FP32 (f32x2: one instruction for both pairs,
+// each element rounded as the scalar operation is). The displacement is taken
+// as p_j - p_i, the exact negation of pair_r2's p_i - p_j; the minimum image
+// is odd in d (rint rounds ties to even, which is symmetric), so the squared
+// distance and the crowder energy equal pair_r2's and crowd_energy's.
+struct PackedBox {
+  float2 iL, nL, M, nM;  // 1/L, -L, +-1.5 * 2^23
+};
+__device__ __forceinline__ PackedBox packed_box(float L, float invL) {
+  const float kMagic = 12582912.0f;  // 1.5 * 2^23, as in min_image
+  return PackedBox{make_float2(invL, invL), make_float2(-L, -L), make_float2(kMagic, kMagic),
+                   make_float2(-kMagic, -kMagic)};
+}
+__device__ __forceinline__ float2 min_image2(float2 d, const PackedBox& B) {
+  return __ffma2_rn(B.nL, __fadd2_rn(__ffma2_rn(d, B.iL, B.M), B.nM), d);
+}
+// squared minimum-image distance from p_i (given negated, npx = (-x_i, -x_i)
+// and so on) to two j beads
+__device__ __forceinline__ float2 pair_r2_2(float2 xj, float2 yj, float2 zj, float2 npx,
+                                            float2 npy, float2 npz, const PackedBox& B) {
+  const float2 ex = min_image2(__fadd2_rn(xj, npx), B);
+  const float2 ey = min_image2(__fadd2_rn(yj, npy), B);
+  const float2 ez = min_image2(__fadd2_rn(zj, npz), B);
+  return __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
+}
+template <bool R12, bool CUT>
+__device__ __forceinline__ float2 crowd_energy2(float2 r2, float2 A, float2 cut2) {
+  const float2 rinv = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
+  const float2 rinv2 = __fmul2_rn(rinv, rinv);
+  const float2 i6 = __fmul2_rn(__fmul2_rn(rinv2, rinv2), rinv2);
+  float2 e = __fmul2_rn(A, i6);
+  if (R12) e = __fmul2_rn(e, i6);
+  if (CUT) {
+    e.x = (r2.x < cut2.x) ? e.x : 0.0f;
+    e.y = (r2.y < cut2.y) ? e.y : 0.0f;
+  }
+  return e;
+}
+
 // ---------------------------------------------------------------- moves
 // Exact-rounding (no FMA contraction) restatement of the reference's rigid-move
 // arithmetic so device trajectories round exactly like the host engine's:

@@ -863,24 +863,79 @@ struct TileItem {
 
 constexpr int kTile = 128;
 
-// Energy of bead i (position pi, type ta) against the j beads s_j[lo-j0 ..
-// hi-j0) of the tile, in ascending j, leaving out the beads [xa, xb) of its own
-// molecule. Beads are stored chains first, crowders after, so the range
-// splits into a chain part [lo, ncb) and a crowder part [ncb, hi), and each
-// part runs a loop specialised to its pair class:
+// Crowder-wall energy of bead i against the tile's beads [a, b), added to acc
+// in ascending j: two beads per pass in packed FP32 from the tile's
+// coordinate arrays (an odd first bead, and a last one, alone). FIXED: one
+// table entry for every j (crowders of the system's one species), else the
+// entry of each j's type.
+template <bool R12, bool CUT, bool FIXED>
+__device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const float* __restrict__ sy,
+                                          const float* __restrict__ sz, const int* __restrict__ st,
+                                          const float4* __restrict__ s_tab, int ta, float4 Tfix,
+                                          int j0, int a, int b, float4 pi, float2 npx, float2 npy,
+                                          float2 npz, const PackedBox& B, float box, float invbox,
+                                          float& acc) {
+  int j = a;
+  if (j < b && ((j - j0) & 1)) {
+    const int o = j - j0;
+    const float4 T = FIXED ? Tfix : s_tab[st[o] * kNT + ta];
+    acc += crowd_energy<R12, CUT>(pair_r2(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
+                                  T.x, T.z);
+    ++j;
+  }
+  const float2 Af = make_float2(Tfix.x, Tfix.x), Cf = make_float2(Tfix.z, Tfix.z);
+#pragma unroll 2
+  for (; j + 1 < b; j += 2) {
+    const int o = j - j0;  // even: 8-byte aligned pairs
+    const float2 r2 = pair_r2_2(*reinterpret_cast<const float2*>(sx + o),
+                                *reinterpret_cast<const float2*>(sy + o),
+                                *reinterpret_cast<const float2*>(sz + o), npx, npy, npz, B);
+    float2 A2 = Af, C2 = Cf;
+    if (!FIXED) {
+      const float4 Ta = s_tab[st[o] * kNT + ta], Tb = s_tab[st[o + 1] * kNT + ta];
+      A2 = make_float2(Ta.x, Tb.x);
+      C2 = make_float2(Ta.z, Tb.z);
+    }
+    const float2 e = crowd_energy2<R12, CUT>(r2, A2, C2);
+    acc += e.x;
+    acc += e.y;
+  }
+  if (j < b) {
+    const int o = j - j0;
+    const float4 T = FIXED ? Tfix : s_tab[st[o] * kNT + ta];
+    acc += crowd_energy<R12, CUT>(pair_r2(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
+                                  T.x, T.z);
+  }
+}
+
+// Energy of bead i (position pi, type ta) against the j beads [lo, hi) of the
+// tile (s_j, and by coordinate sx, sy, sz with types st), in ascending j,
+// leaving out the beads [xa, xb) of its own molecule. Beads are stored chains
+// first, crowders after, so the range splits into a chain part [lo, ncb) and a
+// crowder part [ncb, hi), and each part runs a loop specialised to its pair
+// class:
 //   chain i, chain j ..... Kim-Hummer + Debye-Hueckel, table entry per pair
 //                          (added to the chain-chain sum as well);
 //   any i, crowder j ..... crowder wall with the table entry fixed per i when
 //                          the system has one crowder species;
 //   crowder i, chain j ... crowder wall, table entry per residue type.
-// The single accumulator runs in ascending j, as one unspecialised loop would.
+// The crowder-wall loops take two beads per pass in packed FP32. The single
+// accumulator runs in ascending j, as one unspecialised loop would.
 template <bool R12, bool CUT>
-__device__ __forceinline__ void energy_row(const float4* __restrict__ s_j, int j0, int lo, int hi,
+__device__ __forceinline__ void energy_row(const float4* __restrict__ s_j,
+                                           const float* __restrict__ sx,
+                                           const float* __restrict__ sy,
+                                           const float* __restrict__ sz,
+                                           const int* __restrict__ st, int j0, int lo, int hi,
                                            int xa, int xb, int ncb, int ctype, float4 pi, int ta,
                                            const float4* __restrict__ s_tab, float box,
                                            float invbox, const EnergyConsts& K, float& acc,
                                            float& acc_cc) {
   const bool a_crowd = ta >= kNumAmino;
+  const PackedBox B = packed_box(box, invbox);
+  const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+               npz = make_float2(-pi.z, -pi.z);
+  const float4 Tc = s_tab[(ctype >= 0 ? ctype : 0) * kNT + ta];
   // two sub-ranges of [lo, hi) outside the own molecule
   const int r0a = lo, r0b = min(hi, xa);
   const int r1a = max(lo, xb), r1b = hi;
@@ -898,26 +953,16 @@ __device__ __forceinline__ void energy_row(const float4* __restrict__ s_j, int j
         acc_cc += e;
       }
     } else {
-#pragma unroll 4
-      for (int j = a; j < cb; ++j) {
-        const float4 pj = s_j[j - j0];
-        const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
-        acc += crowd_energy<R12, CUT>(pair_r2(pi, pj, box, invbox), T.x, T.z);
-      }
+      crowd_run<R12, CUT, false>(sx, sy, sz, st, s_tab, ta, Tc, j0, a, cb, pi, npx, npy, npz, B,
+                                 box, invbox, acc);
     }
     const int ca = max(a, ncb);
-    if (ctype >= 0) {
-      const float4 T = s_tab[ctype * kNT + ta];
-#pragma unroll 4
-      for (int j = ca; j < b; ++j)
-        acc += crowd_energy<R12, CUT>(pair_r2(pi, s_j[j - j0], box, invbox), T.x, T.z);
-    } else {
-      for (int j = ca; j < b; ++j) {
-        const float4 pj = s_j[j - j0];
-        const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
-        acc += crowd_energy<R12, CUT>(pair_r2(pi, pj, box, invbox), T.x, T.z);
-      }
-    }
+    if (ctype >= 0)
+      crowd_run<R12, CUT, true>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
+                                box, invbox, acc);
+    else
+      crowd_run<R12, CUT, false>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
+                                 box, invbox, acc);
   }
 }
 
@@ -925,6 +970,24 @@ __device__ __forceinline__ void energy_row(const float4* __restrict__ s_j, int j
 // while); reaching the limit means the copy never completed.
 constexpr int kWaitLimit = 1 << 22;
 
+// Location of an item's j-tile in pos (contiguous, 16-byte aligned, 16 bytes
+// per bead).
+__device__ __forceinline__ const float4* tile_src(const SysDev* __restrict__ sys,
+                                                  const int* __restrict__ inst_sys,
+                                                  const float4* __restrict__ pos, TileItem W,
+                                                  unsigned* bytes) {
+  const SysDev S = sys[inst_sys[W.inst]];
+  const int N = S.n_beads;
+  const int j0 = W.tj * kTile;
+  *bytes = 16u * (unsigned)min(kTile, N - j0);
+  return pos + S.bead_base + (W.inst - S.inst0) * N + j0;
+}
+
+// Two-stage pipeline over the CTA's items: while item k is computed, the
+// bulk copy (TMA, no multicast) of item k+1's j-tile lands in the other
+// buffer, and each thread's i-bead loads are issued before it waits for its
+// own tile. A buffer is refilled only after the barrier that ends the item
+// which read it.
 __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
@@ -932,52 +995,95 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K,
     int* __restrict__ err) {
   __shared__ float4 s_tab[kNT * kNT];
-  __shared__ __align__(128) float4 s_j[kTile];
+  __shared__ __align__(128) float4 s_j[2][kTile];                         // two stages
+  __shared__ __align__(16) float s_jx[kTile], s_jy[kTile], s_jz[kTile];  // the tile by coordinate
+  __shared__ int s_jt[kTile];                                              // and its bead types
   __shared__ double s_red[kTile / 32];
   __shared__ double s_red_cc[kTile / 32];
-  __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ __align__(8) unsigned long long s_bar[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
-  if (tid == 0) mbar_init(&s_bar, 1);
-  unsigned phase = 0;
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    if ((int)blockIdx.x < n_items) {
+      unsigned bytes;
+      const float4* src = tile_src(sys, inst_sys, pos, items[blockIdx.x], &bytes);
+      bulk_load(s_j[0], src, bytes, &s_bar[0]);
+    }
+  }
+  __syncthreads();  // barriers initialised
+  unsigned phases = 0;  // bit b: parity of buffer b's next completion
+  int buf = 0;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x, buf ^= 1) {
     const TileItem W = items[it];
     const SysDev S = sys[inst_sys[W.inst]];
     const int N = S.n_beads;
     const int base = S.bead_base + (W.inst - S.inst0) * N;
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
-    __syncthreads();  // previous item done with s_j (and the barrier initialised)
-    // the j-tile (contiguous, 16-byte aligned, 16 bytes per bead) by one bulk copy
-    if (tid == 0) bulk_load(s_j, pos + base + j0, 16u * (unsigned)jn, &s_bar);
-    const bool ok = mbar_wait(&s_bar, phase, kWaitLimit);
-    phase ^= 1u;
+    // this thread's i bead, loaded while the tile is still in flight
+    const int i = W.ti * kTile + tid;
+    const bool ivalid = i < N;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int xa = 0, xb = 0;
+    if (ivalid) {
+      pi = pos[base + i];
+      const int mi = bead_mol(pi.w);
+      xa = mol_start[S.mstart_off + mi];
+      xb = mol_start[S.mstart_off + mi + 1];
+    }
+    // the next item's tile into the other buffer (its last reader, the
+    // previous item, ended at that item's final barrier)
+    const int next = it + (int)gridDim.x;
+    if (tid == 0 && next < n_items) {
+      unsigned bytes;
+      const float4* src = tile_src(sys, inst_sys, pos, items[next], &bytes);
+      bulk_load(s_j[buf ^ 1], src, bytes, &s_bar[buf ^ 1]);
+    }
+    const bool ok = mbar_wait(&s_bar[buf], (phases >> buf) & 1u, kWaitLimit);
+    phases ^= 1u << buf;
     if (__syncthreads_or(!ok)) {  // the copy never landed: report and stop
-      if (tid == 0) atomicOr(err, 1);
+      if (tid == 0) {
+        atomicOr(err, 1);
+        // the next tile's copy writes this CTA's shared memory: let it land
+        // (bounded) before the CTA leaves
+        if (next < n_items) mbar_wait(&s_bar[buf ^ 1], (phases >> (buf ^ 1)) & 1u, kWaitLimit);
+      }
       return;
     }
-    const int i = W.ti * kTile + tid;
+    const float4* tile = s_j[buf];
+    if (tid < jn) {
+      const float4 p = tile[tid];
+      s_jx[tid] = p.x;
+      s_jy[tid] = p.y;
+      s_jz[tid] = p.z;
+      s_jt[tid] = bead_type(p.w);
+    }
+    __syncthreads();
     double dsum = 0.0, dcc = 0.0;
-    if (i < N) {
-      const float4 pi = pos[base + i];
-      const int ta = bead_type(pi.w), mi = bead_mol(pi.w);
-      const int xa = mol_start[S.mstart_off + mi], xb = mol_start[S.mstart_off + mi + 1];
+    if (ivalid) {
+      const int ta = bead_type(pi.w);
       const int lo = (W.ti == W.tj) ? i + 1 : j0;
       float acc = 0.0f, acc_cc = 0.0f;  // all pairs; chain-chain pairs
       if (K.crowder_mode) {
         if (K.crowder_cut)
-          energy_row<true, true>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
-                                 pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+          energy_row<true, true>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
+                                 S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
+                                 acc, acc_cc);
         else
-          energy_row<true, false>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
-                                  pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+          energy_row<true, false>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
+                                  S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
+                                  acc, acc_cc);
       } else {
         if (K.crowder_cut)
-          energy_row<false, true>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
-                                  pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+          energy_row<false, true>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
+                                  S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
+                                  acc, acc_cc);
         else
-          energy_row<false, false>(s_j, j0, lo, j0 + jn, xa, xb, S.n_chain_beads, S.crowd_type,
-                                   pi, ta, s_tab, S.box, S.invbox, K, acc, acc_cc);
+          energy_row<false, false>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
+                                   S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox,
+                                   K, acc, acc_cc);
       }
       dsum = (double)acc;
       dcc = (double)acc_cc;
@@ -988,7 +1094,7 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
       s_red[warp] = dsum;
       s_red_cc[warp] = dcc;
     }
-    __syncthreads();
+    __syncthreads();  // ends the item: its tile buffer and coordinate arrays are free
     if (tid == 0) {
       double v = 0.0, c = 0.0;
       for (int w = 0; w < kTile / 32; ++w) {
