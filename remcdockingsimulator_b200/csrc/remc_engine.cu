@@ -430,9 +430,21 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     }
     float nc0 = c0, nc1 = c1, nc2 = c2;
     if (!rec.rotate) {
-      nc0 = wrap_box(__fadd_rn(__fadd_rn(c0, rec.t[0]), box), box);
-      nc1 = wrap_box(__fadd_rn(__fadd_rn(c1, rec.t[1]), box), box);
-      nc2 = wrap_box(__fadd_rn(__fadd_rn(c2, rec.t[2]), box), box);
+      const float x0 = __fadd_rn(__fadd_rn(c0, rec.t[0]), box);
+      const float x1 = __fadd_rn(__fadd_rn(c1, rec.t[1]), box);
+      const float x2 = __fadd_rn(__fadd_rn(c2, rec.t[2]), box);
+      // c + t + L almost always lies in [0, 2L), where wrap_box subtracts L
+      // or nothing: one test for all three, selects instead of branches
+      const float L2 = 2.0f * box;  // exact
+      if (x0 >= 0.0f && x0 < L2 && x1 >= 0.0f && x1 < L2 && x2 >= 0.0f && x2 < L2) {
+        nc0 = x0 < box ? x0 : __fsub_rn(x0, box);
+        nc1 = x1 < box ? x1 : __fsub_rn(x1, box);
+        nc2 = x2 < box ? x2 : __fsub_rn(x2, box);
+      } else {
+        nc0 = wrap_box(x0, box);
+        nc1 = wrap_box(x1, box);
+        nc2 = wrap_box(x2, box);
+      }
     }
     // a one-bead rotation moves nothing (its bead sits at the centre): dE = 0
     const bool skip = rec.rotate && n == 1;
@@ -673,33 +685,30 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           if (rec.rotate) A.rel[bead_off + j] = s_trel[b * A.lmax + (j - m0)];
         }
       }
-      if (tid == 0) {
-        if (acc == 1) ++n_neg; else ++n_boltz;
-        if (rec.rotate) {
-          if (crank == 0) {
-          double* qd = A.quat + 4 * (size_t)(mol_off + m);
-          double out[4];
-          quat_mul(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3], qd[0], qd[1], qd[2], qd[3], out);
-          qd[0] = out[0];
-          qd[1] = out[1];
-          qd[2] = out[2];
-          qd[3] = out[3];
-          }
-        } else {
-          cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
-        }
+      if (tid == 0 && rec.rotate && crank == 0) {
+        double* qd = A.quat + 4 * (size_t)(mol_off + m);
+        double out[4];
+        quat_mul(recs_.q[0], recs_.q[1], recs_.q[2], recs_.q[3], qd[0], qd[1], qd[2], qd[3], out);
+        qd[0] = out[0];
+        qd[1] = out[1];
+        qd[2] = out[2];
+        qd[3] = out[3];
       }
-    } else if (tid == 0) {
-      ++n_rej;
+      if (tid == 0 && !rec.rotate) cent[m] = make_float4(nc0, nc1, nc2, 0.0f);
     }
-    if (tid == 0 && !skip) {
+    // counters: every thread keeps them (no branch on the thread index);
+    // thread 0 of rank 0 writes them out
+    n_neg += acc == 1;
+    n_boltz += acc == 2;
+    n_rej += acc == 0;
+    if (!skip) {
       // two evaluations (old and new position) per pair
-      const unsigned long long nn = (unsigned long long)n;
+      const unsigned nn2 = 2u * (unsigned)n;
       if (rec.crowd) {
-        ev_crowd += 2ull * nn * (unsigned long long)(N - n);
+        ev_crowd += (unsigned long long)nn2 * (unsigned)(N - n);
       } else {
-        ev_kh += 2ull * nn * (unsigned long long)(S.n_chain_beads - n);
-        ev_crowd += 2ull * nn * (unsigned long long)(N - S.n_chain_beads);
+        ev_kh += (unsigned long long)nn2 * (unsigned)(S.n_chain_beads - n);
+        ev_crowd += (unsigned long long)nn2 * (unsigned)(N - S.n_chain_beads);
       }
     }
     // ---- Replica::sample at the end of every sampling chunk (main.cpp:975-989):
@@ -710,10 +719,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       if (label >= A.sample_after) {
         const double enc = (ncb < N) ? energy + ecc : energy;
         const bool bound = enc < A.bound_thr;
-        if (tid == 0) {
-          ++n_samp;
-          n_bnd += bound ? 1 : 0;
-        }
+        ++n_samp;  // every thread; thread 0 of rank 0 writes them out
+        n_bnd += bound ? 1 : 0;
         if (bound && A.sample_out && crank == 0) {
           __syncthreads();  // this step's centre / rotation writes visible
           if (tid == 0) {
