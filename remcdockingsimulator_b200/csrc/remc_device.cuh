@@ -202,6 +202,28 @@ __device__ __forceinline__ float2 crowd_energy2(float2 r2, float2 A, float2 cut2
   return e;
 }
 
+// Kim-Hummer + Debye-Hueckel energy of two residue pairs that share the table
+// entry T (the moved bead's new and old position against one bead j), in
+// packed FP32: pair_energy_r2's operations for a residue pair, each product
+// and sum rounded on its own.
+__device__ __forceinline__ float2 kh_energy2(float2 r2, float4 T, float c_xi) {
+  const float2 rinv = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
+  const float2 rinv2 = __fmul2_rn(rinv, rinv);
+  const float2 s2 = __fmul2_rn(make_float2(T.y, T.y), rinv2);
+  const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+  const float2 g = __ffma2_rn(make_float2(-s6.x, -s6.y), s6, s6);  // s6 (1 - s6)
+  float2 lj = __fmul2_rn(make_float2(T.x, T.x), g);
+  const float2 ljr =
+      __ffma2_rn(make_float2(0.5f, 0.5f), make_float2(T.x, T.x), make_float2(-lj.x, -lj.y));
+  lj.x = (r2.x < T.z) ? ljr.x : lj.x;  // repulsive branch: 2 eps' - LJ
+  lj.y = (r2.y < T.z) ? ljr.y : lj.y;
+  const float2 r = __fmul2_rn(r2, rinv);
+  const float2 arg = __fmul2_rn(r, make_float2(c_xi, c_xi));
+  const float2 ex = make_float2(fast_ex2(arg.x), fast_ex2(arg.y));
+  const float2 dh = __fmul2_rn(__fmul2_rn(make_float2(T.w, T.w), ex), rinv);
+  return __fadd2_rn(lj, dh);
+}
+
 // ---------------------------------------------------------------- moves
 // Exact-rounding (no FMA contraction) restatement of the reference's rigid-move
 // arithmetic so device trajectories round exactly like the host engine's:

@@ -551,20 +551,27 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           const int cb = min(hi, ncb);
           int j = lo + ((gtid - lo) & gmask);
           if (!rec.crowd) {
+            // residue pairs: the new and the old evaluation of a pair as the
+            // two lanes of packed FP32
+            const PackedBox PB = packed_box(box, invbox);
             for (; j + gstride < cb; j += 2 * gstride) {
               const float4 pa = s_beads[j], pb = s_beads[j + gstride];
               const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+              const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
+                           naz = make_float2(-pa.z, -pa.z);
+              const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
+                           nbz = make_float2(-pb.z, -pb.z);
               float a = 0.0f, c = 0.0f;
               for (int k = 0; k < n; ++k) {
                 const float4 po = oldp[k], pn = newp[k];
+                const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
+                             kz = make_float2(pn.z, po.z);
                 const float4* row = s_tab + bead_type(po.w) * kNT;
                 const float4 Ta = row[ta], Tb = row[tb];
-                const float ena = pair_energy_r2(pair_r2(pn, pa, box, invbox), Ta, false, A.K);
-                const float eoa = pair_energy_r2(pair_r2(po, pa, box, invbox), Ta, false, A.K);
-                const float enb = pair_energy_r2(pair_r2(pn, pb, box, invbox), Tb, false, A.K);
-                const float eob = pair_energy_r2(pair_r2(po, pb, box, invbox), Tb, false, A.K);
-                a += ena - eoa;
-                c += enb - eob;
+                const float2 ea = kh_energy2(pair_r2_2(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
+                const float2 eb = kh_energy2(pair_r2_2(kx, ky, kz, nbx, nby, nbz, PB), Tb, A.K.c_xi);
+                a += ea.x - ea.y;
+                c += eb.x - eb.y;
               }
               acc_c += a;
               acc_c += c;
@@ -595,21 +602,30 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             }
           }
           const bool one_ct = ctype >= 0;
+          const PackedBox PBc = packed_box(box, invbox);
           for (; j + gstride < hi; j += 2 * gstride) {
             const float4 pa = s_beads[j], pb = s_beads[j + gstride];
             const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+            const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
+                         naz = make_float2(-pa.z, -pa.z);
+            const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
+                         nbz = make_float2(-pb.z, -pb.z);
             float a = 0.0f, c = 0.0f;
             for (int k = 0; k < n; ++k) {
               const float4 po = oldp[k], pn = newp[k];
+              const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
+                           kz = make_float2(pn.z, po.z);
               const float4* row = s_tab + bead_type(po.w) * kNT;
               const float4 Ta = row[ta];
               const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
-              const float ena = crowd_energy<R12, CUT>(pair_r2(pn, pa, box, invbox), Ta.x, Ta.z);
-              const float eoa = crowd_energy<R12, CUT>(pair_r2(po, pa, box, invbox), Ta.x, Ta.z);
-              const float enb = crowd_energy<R12, CUT>(pair_r2(pn, pb, box, invbox), Tb.x, Tb.z);
-              const float eob = crowd_energy<R12, CUT>(pair_r2(po, pb, box, invbox), Tb.x, Tb.z);
-              a += ena - eoa;
-              c += enb - eob;
+              const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2(kx, ky, kz, nax, nay, naz, PBc),
+                                                        make_float2(Ta.x, Ta.x),
+                                                        make_float2(Ta.z, Ta.z));
+              const float2 eb = crowd_energy2<R12, CUT>(pair_r2_2(kx, ky, kz, nbx, nby, nbz, PBc),
+                                                        make_float2(Tb.x, Tb.x),
+                                                        make_float2(Tb.z, Tb.z));
+              a += ea.x - ea.y;
+              c += eb.x - eb.y;
             }
             acc_o += a;
             acc_o += c;
