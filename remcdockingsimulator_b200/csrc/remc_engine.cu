@@ -493,18 +493,27 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           // bead itself (j = m0) left out of the sum
           const bool one_ct = ctype >= 0;
           const float4 Tc = trow[one_ct ? ctype : 0];
+          // the two beads of a pass as the two lanes of packed FP32, against
+          // the moved bead's new and old position (negated once per step)
+          const PackedBox PB1 = packed_box(box, invbox);
+          const float2 nnx = make_float2(-pnew1.x, -pnew1.x), nny = make_float2(-pnew1.y, -pnew1.y),
+                       nnz = make_float2(-pnew1.z, -pnew1.z);
+          const float2 nox = make_float2(-pold1.x, -pold1.x), noy = make_float2(-pold1.y, -pold1.y),
+                       noz = make_float2(-pold1.z, -pold1.z);
           int j = gtid;
           for (; j + gstride < N; j += 2 * gstride) {
             const int j2 = j + gstride;
             const float4 pa = s_beads[j], pb = s_beads[j2];
             const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
             const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trow[bead_type(pb.w)];
-            const float ena = crowd_energy<R12, CUT>(pair_r2(pnew1, pa, box, invbox), Ta.x, Ta.z);
-            const float eoa = crowd_energy<R12, CUT>(pair_r2(pold1, pa, box, invbox), Ta.x, Ta.z);
-            const float enb = crowd_energy<R12, CUT>(pair_r2(pnew1, pb, box, invbox), Tb.x, Tb.z);
-            const float eob = crowd_energy<R12, CUT>(pair_r2(pold1, pb, box, invbox), Tb.x, Tb.z);
-            if (j != m0) acc_o += ena - eoa;
-            if (j2 != m0) acc_o += enb - eob;
+            const float2 xj = make_float2(pa.x, pb.x), yj = make_float2(pa.y, pb.y),
+                         zj = make_float2(pa.z, pb.z);
+            const float2 A2 = make_float2(Ta.x, Tb.x), C2 = make_float2(Ta.z, Tb.z);
+            const float2 en = crowd_energy2<R12, CUT>(pair_r2_2(xj, yj, zj, nnx, nny, nnz, PB1), A2, C2);
+            const float2 eo = crowd_energy2<R12, CUT>(pair_r2_2(xj, yj, zj, nox, noy, noz, PB1), A2, C2);
+            const float2 d = __fadd2_rn(en, make_float2(-eo.x, -eo.y));
+            if (j != m0) acc_o += d.x;
+            if (j2 != m0) acc_o += d.y;
           }
           if (j < N && j != m0) {
             const float4 pa = s_beads[j];
