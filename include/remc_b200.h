@@ -235,6 +235,13 @@ int remc_set_bead_storage(remc_handle* h, int in_shared_memory);
 int remc_get_bead_storage(remc_handle* h, int* in_shared_memory);
 
 int remc_sync(remc_handle* h);
+/* Failure-path check: runs one warp whose bounded device-side wait (the one
+ * the energy kernel uses for its tile copies) waits for something that never
+ * happens, gives up after `polls` polls (1 .. 2^20) and sets the handle's
+ * error word. Returns REMC_ERR_TIMEOUT, as a call whose tile copy never
+ * landed would; the handle stays usable. No reference counterpart (the
+ * reference aborts through cutil on device errors). */
+int remc_check_wait_timeout(remc_handle* h, int polls);
 int remc_num_instances(const remc_handle* h);
 const char* remc_last_error_string(void);
 

@@ -1139,6 +1139,18 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
   }
 }
 
+// One warp waits, with the energy kernel's bounded mbarrier wait, for a
+// phase that nothing completes (no copy is issued, nothing arrives): after
+// `polls` polls the wait gives up and the error word is set, as when a tile's
+// bulk copy never lands. Nothing is in flight when the kernel returns.
+__global__ void wait_probe_kernel(int* __restrict__ err, int polls) {
+  __shared__ __align__(8) unsigned long long s_bar;
+  if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+  __syncthreads();
+  const bool ok = mbar_wait(&s_bar, 0u, polls);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, 1);
+}
+
 // Per-instance fixed-order sum of the tile partials.
 __global__ void energy_reduce_kernel(const int* __restrict__ item_off, int n_inst,
                                      const double* __restrict__ scratch,
@@ -3054,6 +3066,15 @@ int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* clust
   if (mol_in_smem) *mol_in_smem = h->mol_in_smem;
   if (cluster) *cluster = h->sweep_csize;
   return REMC_OK;
+}
+
+int remc_check_wait_timeout(remc_handle* h, int polls) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (polls < 1 || polls > (1 << 20))
+    return set_error(REMC_ERR_INVALID, "polls must be in [1, 2^20]");
+  wait_probe_kernel<<<1, 32, 0, h->stream>>>(h->d_err, polls);
+  REMC_CUDA_TRY(cudaGetLastError());
+  return check_device_error(h);
 }
 
 int remc_sync(remc_handle* h) {
