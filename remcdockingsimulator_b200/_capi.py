@@ -97,6 +97,7 @@ _SIGS = {
     "remc_set_bead_storage": (C.c_int, [P, C.c_int]),
     "remc_get_bead_storage": (C.c_int, [P, PI]),
     "remc_check_wait_timeout": (C.c_int, [P, C.c_int]),
+    "remc_get_fold_flags": (C.c_int, [P, PI]),
     "remc_last_error_string": (C.c_char_p, []),
     "remc_post_rebuild": (C.c_int, [PF, PI, C.c_int, PI, PF, C.c_float, PD, PF, C.c_int, PF, PF]),
     "remc_post_drms": (C.c_int, [PF, C.c_int, PF, PI, C.c_int, C.c_int, C.c_float, C.c_float, PD,

@@ -169,23 +169,43 @@ __device__ __forceinline__ float pair_r2(float4 a, float4 b, float L, float invL
 // is odd in d (rint rounds ties to even, which is symmetric), so the squared
 // distance and the crowder energy equal pair_r2's and crowd_energy's.
 struct PackedBox {
-  float2 iL, nL, M, nM;  // 1/L, -L, +-1.5 * 2^23
+  float2 iL, nL, M, nM, L;  // 1/L, -L, +-1.5 * 2^23, L
 };
 __device__ __forceinline__ PackedBox packed_box(float L, float invL) {
   const float kMagic = 12582912.0f;  // 1.5 * 2^23, as in min_image
   return PackedBox{make_float2(invL, invL), make_float2(-L, -L), make_float2(kMagic, kMagic),
-                   make_float2(-kMagic, -kMagic)};
+                   make_float2(-kMagic, -kMagic), make_float2(L, L)};
 }
 __device__ __forceinline__ float2 min_image2(float2 d, const PackedBox& B) {
   return __ffma2_rn(B.nL, __fadd2_rn(__ffma2_rn(d, B.iL, B.M), B.nM), d);
 }
+// The minimum image folded: for |d| < 1.5 L the nearer image is at distance
+// min(|d|, L - |d|) in magnitude (negative past L, where the square is still
+// right), one add on the FMA pipe and a min instead of three FMA-pipe
+// operations. L - |d| is rounded once, as d -+ L is in min_image, so the
+// result equals min_image's in magnitude except where d/L lies within a
+// rounding of +-1/2, where both images are half a box away. Only for systems
+// whose every bead pair is known to satisfy |d| < 1.5 L.
+__device__ __forceinline__ float2 fold_image2(float2 d, const PackedBox& B) {
+  const float2 a = make_float2(fabsf(d.x), fabsf(d.y));
+  const float2 t = __fadd2_rn(B.L, make_float2(-a.x, -a.y));
+  return make_float2(fminf(a.x, t.x), fminf(a.y, t.y));
+}
 // squared minimum-image distance from p_i (given negated, npx = (-x_i, -x_i)
-// and so on) to two j beads
+// and so on) to two j beads; FOLD: fold_image2 (the caller knows |d| < 1.5 L)
+template <bool FOLD = false>
 __device__ __forceinline__ float2 pair_r2_2(float2 xj, float2 yj, float2 zj, float2 npx,
                                             float2 npy, float2 npz, const PackedBox& B) {
-  const float2 ex = min_image2(__fadd2_rn(xj, npx), B);
-  const float2 ey = min_image2(__fadd2_rn(yj, npy), B);
-  const float2 ez = min_image2(__fadd2_rn(zj, npz), B);
+  float2 ex = __fadd2_rn(xj, npx), ey = __fadd2_rn(yj, npy), ez = __fadd2_rn(zj, npz);
+  if constexpr (FOLD) {
+    ex = fold_image2(ex, B);
+    ey = fold_image2(ey, B);
+    ez = fold_image2(ez, B);
+  } else {
+    ex = min_image2(ex, B);
+    ey = min_image2(ey, B);
+    ez = min_image2(ez, B);
+  }
   return __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
 }
 template <bool R12, bool CUT>

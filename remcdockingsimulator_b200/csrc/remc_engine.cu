@@ -34,6 +34,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "remc_device.cuh"
@@ -75,6 +76,11 @@ struct SysDev {
   int translate_only_crowders;
   int n_chain_beads;  // beads of residue type; the rest are crowders
   int crowd_type;     // the one bead type of every crowder, or -1 (none or mixed)
+  // 1: every bead pair is within 1.5 box lengths on each axis, for the state
+  // uploaded last and every state the sweep can reach from it (set on the
+  // device by fold_flag_kernel at each upload; the sweep then folds the
+  // minimum image)
+  int fold_mi;
 };
 
 // Per-step proposal record: everything about step s of one replica that does
@@ -501,6 +507,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           const float2 nox = make_float2(-pold1.x, -pold1.x), noy = make_float2(-pold1.y, -pold1.y),
                        noz = make_float2(-pold1.z, -pold1.z);
           int j = gtid;
+          // folded minimum image where the system allows it (fold_mi)
+          auto pass1 = [&](auto fold) {
+          constexpr bool F = decltype(fold)::value;
           for (; j + gstride < N; j += 2 * gstride) {
             const int j2 = j + gstride;
             const float4 pa = s_beads[j], pb = s_beads[j2];
@@ -509,12 +518,16 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             const float2 xj = make_float2(pa.x, pb.x), yj = make_float2(pa.y, pb.y),
                          zj = make_float2(pa.z, pb.z);
             const float2 A2 = make_float2(Ta.x, Tb.x), C2 = make_float2(Ta.z, Tb.z);
-            const float2 en = crowd_energy2<R12, CUT>(pair_r2_2(xj, yj, zj, nnx, nny, nnz, PB1), A2, C2);
-            const float2 eo = crowd_energy2<R12, CUT>(pair_r2_2(xj, yj, zj, nox, noy, noz, PB1), A2, C2);
+            const float2 en =
+                crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nnx, nny, nnz, PB1), A2, C2);
+            const float2 eo =
+                crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nox, noy, noz, PB1), A2, C2);
             const float2 d = __fadd2_rn(en, make_float2(-eo.x, -eo.y));
             if (j != m0) acc_o += d.x;
             if (j2 != m0) acc_o += d.y;
           }
+          };
+          if (S.fold_mi) pass1(std::true_type{}); else pass1(std::false_type{});
           if (j < N && j != m0) {
             const float4 pa = s_beads[j];
             const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
@@ -563,6 +576,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             // residue pairs: the new and the old evaluation of a pair as the
             // two lanes of packed FP32
             const PackedBox PB = packed_box(box, invbox);
+            auto pass2 = [&](auto fold) {
+            constexpr bool F = decltype(fold)::value;
             for (; j + gstride < cb; j += 2 * gstride) {
               const float4 pa = s_beads[j], pb = s_beads[j + gstride];
               const int ta = bead_type(pa.w), tb = bead_type(pb.w);
@@ -577,14 +592,18 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
                              kz = make_float2(pn.z, po.z);
                 const float4* row = s_tab + bead_type(po.w) * kNT;
                 const float4 Ta = row[ta], Tb = row[tb];
-                const float2 ea = kh_energy2(pair_r2_2(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
-                const float2 eb = kh_energy2(pair_r2_2(kx, ky, kz, nbx, nby, nbz, PB), Tb, A.K.c_xi);
+                const float2 ea =
+                    kh_energy2(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
+                const float2 eb =
+                    kh_energy2(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PB), Tb, A.K.c_xi);
                 a += ea.x - ea.y;
                 c += eb.x - eb.y;
               }
               acc_c += a;
               acc_c += c;
             }
+            };
+            if (S.fold_mi) pass2(std::true_type{}); else pass2(std::false_type{});
           }
           for (; j < cb; j += gstride) {
             const float4 pj = s_beads[j];
@@ -612,6 +631,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           }
           const bool one_ct = ctype >= 0;
           const PackedBox PBc = packed_box(box, invbox);
+          auto pass3 = [&](auto fold) {
+          constexpr bool F = decltype(fold)::value;
           for (; j + gstride < hi; j += 2 * gstride) {
             const float4 pa = s_beads[j], pb = s_beads[j + gstride];
             const int ta = bead_type(pa.w), tb = bead_type(pb.w);
@@ -627,10 +648,10 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               const float4* row = s_tab + bead_type(po.w) * kNT;
               const float4 Ta = row[ta];
               const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
-              const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2(kx, ky, kz, nax, nay, naz, PBc),
+              const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PBc),
                                                         make_float2(Ta.x, Ta.x),
                                                         make_float2(Ta.z, Ta.z));
-              const float2 eb = crowd_energy2<R12, CUT>(pair_r2_2(kx, ky, kz, nbx, nby, nbz, PBc),
+              const float2 eb = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PBc),
                                                         make_float2(Tb.x, Tb.x),
                                                         make_float2(Tb.z, Tb.z));
               a += ea.x - ea.y;
@@ -639,6 +660,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             acc_o += a;
             acc_o += c;
           }
+          };
+          if (S.fold_mi) pass3(std::true_type{}); else pass3(std::false_type{});
           for (; j < hi; j += gstride) {
             const float4 pj = s_beads[j];
             const int tb = bead_type(pj.w);
@@ -885,6 +908,53 @@ __global__ void state_unpack_kernel(const float4* __restrict__ pos, const float4
     cen3[3 * m] = c.x;
     cen3[3 * m + 1] = c.y;
     cen3[3 * m + 2] = c.z;
+  }
+}
+
+// Per system (one CTA each): may the sweep fold the minimum image? Moves keep
+// every centre in [0, L) (translations wrap it, rotations leave it) and keep
+// each bead's distance R from its centre (a rotation of rel), so on each axis
+// any two beads of different molecules are at most span + 2 R apart, with span
+// the extent of [0, L) and the uploaded centres together and R the largest
+// |rel| over all instances. fold_image2 needs less than 1.5 L; the test keeps
+// a margin (2.02 R, 1.49 L) for the rounding of repeated rotations.
+__global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float4* __restrict__ rel,
+                                 const float4* __restrict__ cent) {
+  __shared__ float s_v[7][32];
+  const SysDev S = sys[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float r2 = 0.0f, lo0 = 0.0f, lo1 = 0.0f, lo2 = 0.0f, hi0 = S.box, hi1 = S.box, hi2 = S.box;
+  const long long nb = (long long)S.n_rep * S.n_beads, nm = (long long)S.n_rep * S.n_mol;
+  for (long long i = tid; i < nb; i += blockDim.x) {
+    const float4 r = rel[S.bead_base + i];
+    r2 = fmaxf(r2, fmaf(r.x, r.x, fmaf(r.y, r.y, r.z * r.z)));
+  }
+  for (long long m = tid; m < nm; m += blockDim.x) {
+    const float4 c = cent[S.mol_base + m];
+    lo0 = fminf(lo0, c.x);
+    lo1 = fminf(lo1, c.y);
+    lo2 = fminf(lo2, c.z);
+    hi0 = fmaxf(hi0, c.x);
+    hi1 = fmaxf(hi1, c.y);
+    hi2 = fmaxf(hi2, c.z);
+  }
+  float v[7] = {r2, -lo0, -lo1, -lo2, hi0, hi1, hi2};  // all reduced by max
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    for (int off = 16; off > 0; off >>= 1) v[k] = fmaxf(v[k], __shfl_down_sync(0xffffffffu, v[k], off));
+    if (lane == 0) s_v[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float w[7];
+    for (int k = 0; k < 7; ++k) {
+      w[k] = s_v[k][0];
+      for (int q = 1; q < (int)(blockDim.x >> 5); ++q) w[k] = fmaxf(w[k], s_v[k][q]);
+    }
+    const float R2 = 2.02f * sqrtf(w[0]), lim = 1.49f * S.box;
+    const bool ok = (w[4] + w[1]) + R2 <= lim && (w[5] + w[2]) + R2 <= lim &&
+                    (w[6] + w[3]) + R2 <= lim;
+    sys[blockIdx.x].fold_mi = ok ? 1 : 0;
   }
 }
 
@@ -2445,6 +2515,8 @@ int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const 
   state_pack_kernel<<<grid, 256, 0, h->stream>>>(sp, sr, sc, h->d_bead_info, (long long)nb,
                                                  (long long)nm, h->d_pos, h->d_rel, h->d_centre);
   REMC_CUDA_TRY(cudaGetLastError());
+  fold_flag_kernel<<<h->n_sys, 256, 0, h->stream>>>(h->d_sys, h->d_rel, h->d_centre);
+  REMC_CUDA_TRY(cudaGetLastError());
   REMC_CUDA_TRY(cudaMemcpyAsync(h->d_quat, h->d_stage_q, sizeof(double) * 4 * nm,
                                 cudaMemcpyDeviceToDevice, h->stream));
   h->state_set = true;
@@ -3065,6 +3137,16 @@ int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* clust
   if (threads) *threads = h->sweep_threads;
   if (mol_in_smem) *mol_in_smem = h->mol_in_smem;
   if (cluster) *cluster = h->sweep_csize;
+  return REMC_OK;
+}
+
+int remc_get_fold_flags(remc_handle* h, int* per_system) {
+  if (!h || !per_system) return set_error(REMC_ERR_INVALID, "null argument");
+  std::vector<SysDev> sd(h->n_sys);
+  REMC_CUDA_TRY(cudaMemcpyAsync(sd.data(), h->d_sys, sizeof(SysDev) * h->n_sys,
+                                cudaMemcpyDeviceToHost, h->stream));
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (int s2 = 0; s2 < h->n_sys; ++s2) per_system[s2] = sd[s2].fold_mi;
   return REMC_OK;
 }
 

@@ -358,6 +358,13 @@ class Engine:
         global memory (False; any system size, same results)."""
         check(lib().remc_set_bead_storage(self._h, 1 if shared else 0))
 
+    def fold_flags(self) -> np.ndarray:
+        """Per system: 1 when the sweep folds the minimum image (see
+        remc_get_fold_flags)."""
+        out = np.zeros(len(self.systems), np.int32)
+        check(lib().remc_get_fold_flags(self._h, _ptr(out, C.c_int)))
+        return out
+
     def beads_in_shared_memory(self) -> bool:
         v = C.c_int()
         check(lib().remc_get_bead_storage(self._h, C.byref(v)))
