@@ -911,34 +911,61 @@ __global__ void state_unpack_kernel(const float4* __restrict__ pos, const float4
   }
 }
 
-// Per system (one CTA each): may the sweep fold the minimum image? Moves keep
-// every centre in [0, L) (translations wrap it, rotations leave it) and keep
-// each bead's distance R from its centre (a rotation of rel), so on each axis
-// any two beads of different molecules are at most span + 2 R apart, with span
-// the extent of [0, L) and the uploaded centres together and R the largest
-// |rel| over all instances. fold_image2 needs less than 1.5 L; the test keeps
-// a margin (2.02 R, 1.49 L) for the rounding of repeated rotations.
-__global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float4* __restrict__ rel,
-                                 const float4* __restrict__ cent) {
+// May the sweep fold the minimum image of a system? Moves keep every centre
+// in [0, L) (translations wrap it, rotations leave it) and keep each bead's
+// distance R from its centre (a rotation of rel), so on each axis any two
+// beads of different molecules are at most span + 2 R apart, with span the
+// extent of [0, L) and the uploaded centres together and R the largest |rel|
+// over all instances. fold_image2 needs less than 1.5 L; the test keeps a
+// margin (2.02 R, 1.49 L) for the rounding of repeated rotations.
+// fold_part_kernel: one CTA per instance, its largest |rel|^2 and centre
+// extent (part[inst][0..6]: R^2, -lo xyz, hi xyz, all combined by max);
+// fold_flag_kernel: one CTA per system combines its instances.
+__global__ void fold_part_kernel(const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
+                                 const float4* __restrict__ rel, const float4* __restrict__ cent,
+                                 float* __restrict__ part) {
+  __shared__ float s_v[7][32];
+  const int inst = blockIdx.x;
+  const SysDev S = sys[inst_sys[inst]];
+  const int slot = inst - S.inst0;
+  const float4* r = rel + S.bead_base + (size_t)slot * S.n_beads;
+  const float4* c = cent + S.mol_base + (size_t)slot * S.n_mol;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float v[7] = {0.0f, 0.0f, 0.0f, 0.0f, S.box, S.box, S.box};
+  for (int i = tid; i < S.n_beads; i += blockDim.x) {
+    const float4 q = r[i];
+    v[0] = fmaxf(v[0], fmaf(q.x, q.x, fmaf(q.y, q.y, q.z * q.z)));
+  }
+  for (int m = tid; m < S.n_mol; m += blockDim.x) {
+    const float4 q = c[m];
+    v[1] = fmaxf(v[1], -q.x);
+    v[2] = fmaxf(v[2], -q.y);
+    v[3] = fmaxf(v[3], -q.z);
+    v[4] = fmaxf(v[4], q.x);
+    v[5] = fmaxf(v[5], q.y);
+    v[6] = fmaxf(v[6], q.z);
+  }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    for (int off = 16; off > 0; off >>= 1) v[k] = fmaxf(v[k], __shfl_down_sync(0xffffffffu, v[k], off));
+    if (lane == 0) s_v[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (tid < 7) {
+    float w = s_v[tid][0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) w = fmaxf(w, s_v[tid][q]);
+    part[(size_t)inst * 8 + tid] = w;
+  }
+}
+
+__global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float* __restrict__ part) {
   __shared__ float s_v[7][32];
   const SysDev S = sys[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float r2 = 0.0f, lo0 = 0.0f, lo1 = 0.0f, lo2 = 0.0f, hi0 = S.box, hi1 = S.box, hi2 = S.box;
-  const long long nb = (long long)S.n_rep * S.n_beads, nm = (long long)S.n_rep * S.n_mol;
-  for (long long i = tid; i < nb; i += blockDim.x) {
-    const float4 r = rel[S.bead_base + i];
-    r2 = fmaxf(r2, fmaf(r.x, r.x, fmaf(r.y, r.y, r.z * r.z)));
-  }
-  for (long long m = tid; m < nm; m += blockDim.x) {
-    const float4 c = cent[S.mol_base + m];
-    lo0 = fminf(lo0, c.x);
-    lo1 = fminf(lo1, c.y);
-    lo2 = fminf(lo2, c.z);
-    hi0 = fmaxf(hi0, c.x);
-    hi1 = fmaxf(hi1, c.y);
-    hi2 = fmaxf(hi2, c.z);
-  }
-  float v[7] = {r2, -lo0, -lo1, -lo2, hi0, hi1, hi2};  // all reduced by max
+  float v[7] = {0.0f, 0.0f, 0.0f, 0.0f, S.box, S.box, S.box};
+  for (int i = tid; i < S.n_rep; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 7; ++k) v[k] = fmaxf(v[k], part[(size_t)(S.inst0 + i) * 8 + k]);
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
     for (int off = 16; off > 0; off >>= 1) v[k] = fmaxf(v[k], __shfl_down_sync(0xffffffffu, v[k], off));
@@ -1760,8 +1787,10 @@ struct remc_handle {
   int sweep_grid = 0;  // resident CTAs of the persistent sweep
   int mol_in_smem = 1; // molecule centres/starts in shared memory (else global)
   int sweep_csize = 1; // CTAs per replica (thread-block cluster size)
+  int sweep_cluster_slots = 0;  // clusters of that size the GPU holds at once
   int beads_in_smem = 1; // beads resident in shared memory (else updated in place in global)
   float4* d_trial_scratch = nullptr;  // trial buffers when the beads stay in global memory
+  float* d_fold_part = nullptr;       // per instance: the fold test's partial extents [8]
   size_t trial_scratch_cap = 0;       // float4 entries
   int max_dyn_smem = 0;
   int config_gen = 0;  // bumped when the sweep schedule changes
@@ -1827,7 +1856,7 @@ void free_all(remc_handle* h) {
                   h->d_dxi,        h->d_eadj,     h->d_mft,
                   h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad,
-                  h->d_err,      h->d_trial_scratch};
+                  h->d_err,      h->d_trial_scratch, h->d_fold_part};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1980,6 +2009,7 @@ int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize, int
     if (e != cudaSuccess || clusters < 1)
       return set_error(REMC_ERR_INVALID, "a cluster of %d sweep CTAs does not fit: %s", csize,
                        cudaGetErrorString(e));
+    h->sweep_cluster_slots = clusters;
   }
   if (!beads_in_smem) {
     // trial buffers of every (instance, CTA rank): 4 lmax float4 each
@@ -2375,6 +2405,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_sample_cursor, 4);
   if (!rc) rc = dev_alloc(&h->d_newpos, h->lmax);
   if (!rc) rc = dev_alloc(&h->d_dE, 1);
+  if (!rc) rc = dev_alloc(&h->d_fold_part, (size_t)h->n_inst * 8);
   auto up = [&](void* dst, const void* src, size_t bytes) {
     if (rc) return;
     cudaError_t ee = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
@@ -2515,7 +2546,10 @@ int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const 
   state_pack_kernel<<<grid, 256, 0, h->stream>>>(sp, sr, sc, h->d_bead_info, (long long)nb,
                                                  (long long)nm, h->d_pos, h->d_rel, h->d_centre);
   REMC_CUDA_TRY(cudaGetLastError());
-  fold_flag_kernel<<<h->n_sys, 256, 0, h->stream>>>(h->d_sys, h->d_rel, h->d_centre);
+  fold_part_kernel<<<h->n_inst, 256, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_rel,
+                                                     h->d_centre, h->d_fold_part);
+  REMC_CUDA_TRY(cudaGetLastError());
+  fold_flag_kernel<<<h->n_sys, 256, 0, h->stream>>>(h->d_sys, h->d_fold_part);
   REMC_CUDA_TRY(cudaGetLastError());
   REMC_CUDA_TRY(cudaMemcpyAsync(h->d_quat, h->d_stage_q, sizeof(double) * 4 * nm,
                                 cudaMemcpyDeviceToDevice, h->stream));
@@ -3061,23 +3095,28 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // beads in shared memory wherever some schedule allows it; in global memory
+  // (any size, slower) only when no schedule does
+  bool any_fit = false;
+  for (int bi = 1; bi >= 0 && !rc && !any_fit; --bi) {
   for (int ci = 0; ci < n_c && !rc; ++ci) {
   for (int ti = 0; ti < 2 && !rc; ++ti) {
     for (int mi = 1; mi >= 0 && !rc; --mi) {
-      // beads in global memory only where they do not fit in shared memory
-      int bi = 1;
-      if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci], 1) != REMC_OK) {
-        if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci], 0) != REMC_OK) continue;
-        bi = 0;
-      }
-      float ms = 0.0f;
-      for (int rep = 0; rep < 2 && !rc; ++rep) {  // first launch warms up
+      if (configure_sweep(h, cand_threads[ti], mi, cand_c[ci], bi) != REMC_OK) continue;
+      // a cluster size whose clusters cannot all be resident would run the
+      // replicas in waves: not a candidate
+      if (cand_c[ci] > 1 && h->n_inst > h->sweep_cluster_slots) continue;
+      any_fit = true;
+      float ms = 1e30f;
+      for (int rep = 0; rep < 3 && !rc; ++rep) {  // first launch warms up; best of two
+        float t_rep = 0.0f;
         cudaEventRecord(e0, h->stream);
         rc = launch_sweep(h, probe_steps, seed, 0, nullptr);
         cudaEventRecord(e1, h->stream);
         if (!rc && cudaEventSynchronize(e1) != cudaSuccess)
           rc = set_error(REMC_ERR_CUDA, "autotune probe failed");
-        if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+        if (!rc) cudaEventElapsedTime(&t_rep, e0, e1);
+        if (!rc && rep > 0) ms = std::min(ms, t_rep);
         for (int i = 0; i < nb && !rc; ++i)
           if (cudaMemcpyAsync(bufs[i].dev, bufs[i].save, bufs[i].bytes, cudaMemcpyDeviceToDevice,
                               h->stream) != cudaSuccess)
@@ -3091,6 +3130,7 @@ int remc_autotune(remc_handle* h, int probe_steps, uint64_t seed, int* threads_o
         best_b = bi;
       }
     }
+  }
   }
   }
   cudaEventDestroy(e0);
