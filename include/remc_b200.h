@@ -233,10 +233,11 @@ int remc_get_schedule(remc_handle* h, int* threads, int* mol_in_smem, int* clust
  * either way. No reference counterpart. */
 int remc_set_bead_storage(remc_handle* h, int in_shared_memory);
 /* Per system, 1 when the sweep folds the minimum image (min(|d|, L - |d|) per
- * axis instead of d - L rint(d/L)): set at every remc_upload_state when the
- * centres' extent, taken together with [0, L), plus twice the largest bead
- * distance from its centre, stays below 1.5 L on every axis (with a margin),
- * so that no bead pair the sweep can reach is 1.5 box lengths apart. Results
+ * axis instead of d - L rint(d/L)): set at every remc_upload_state when, on
+ * every axis, [min(p_min, -R), max(p_max, L + R)] is shorter than 1.5 L (with
+ * a margin), p the uploaded bead positions and R the largest bead distance
+ * from its centre, so that no bead pair the sweep can reach is 1.5 box
+ * lengths apart (moved molecules keep their centre in [0, L)). Results
  * equal the unfolded ones except for pairs half a box apart to within a
  * rounding. No reference counterpart. */
 int remc_get_fold_flags(remc_handle* h, int* per_system);

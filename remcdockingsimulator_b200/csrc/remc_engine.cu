@@ -911,39 +911,35 @@ __global__ void state_unpack_kernel(const float4* __restrict__ pos, const float4
   }
 }
 
-// May the sweep fold the minimum image of a system? Moves keep every centre
-// in [0, L) (translations wrap it, rotations leave it) and keep each bead's
-// distance R from its centre (a rotation of rel), so on each axis any two
-// beads of different molecules are at most span + 2 R apart, with span the
-// extent of [0, L) and the uploaded centres together and R the largest |rel|
-// over all instances. fold_image2 needs less than 1.5 L; the test keeps a
-// margin (2.02 R, 1.49 L) for the rounding of repeated rotations.
-// fold_part_kernel: one CTA per instance, its largest |rel|^2 and centre
-// extent (part[inst][0..6]: R^2, -lo xyz, hi xyz, all combined by max);
-// fold_flag_kernel: one CTA per system combines its instances.
+// May the sweep fold the minimum image of a system? A bead the sweep has not
+// moved is where it was uploaded; a moved molecule has its centre in [0, L)
+// (translations wrap it, rotations leave it) and each bead within R of it (a
+// rotation of rel keeps |rel|), R the largest |rel| over all instances. So on
+// each axis every bead lies in [min(p_min, -R), max(p_max, L + R)], and no two
+// are further apart than that interval is long. fold_image2 needs less than
+// 1.5 L; the test keeps a margin (1.01 R, 1.49 L) for the rounding of repeated
+// rotations. fold_part_kernel: one CTA per instance, its largest |rel|^2 and
+// bead extent (part[inst][0..6]: R^2, -p_min xyz, p_max xyz, all combined by
+// max); fold_flag_kernel: one CTA per system combines its instances.
 __global__ void fold_part_kernel(const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
-                                 const float4* __restrict__ rel, const float4* __restrict__ cent,
+                                 const float4* __restrict__ pos, const float4* __restrict__ rel,
                                  float* __restrict__ part) {
   __shared__ float s_v[7][32];
   const int inst = blockIdx.x;
   const SysDev S = sys[inst_sys[inst]];
-  const int slot = inst - S.inst0;
-  const float4* r = rel + S.bead_base + (size_t)slot * S.n_beads;
-  const float4* c = cent + S.mol_base + (size_t)slot * S.n_mol;
+  const size_t base = S.bead_base + (size_t)(inst - S.inst0) * S.n_beads;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float v[7] = {0.0f, 0.0f, 0.0f, 0.0f, S.box, S.box, S.box};
+  const float lowest = -3.0e38f;
+  float v[7] = {0.0f, lowest, lowest, lowest, lowest, lowest, lowest};
   for (int i = tid; i < S.n_beads; i += blockDim.x) {
-    const float4 q = r[i];
+    const float4 q = rel[base + i], p = pos[base + i];
     v[0] = fmaxf(v[0], fmaf(q.x, q.x, fmaf(q.y, q.y, q.z * q.z)));
-  }
-  for (int m = tid; m < S.n_mol; m += blockDim.x) {
-    const float4 q = c[m];
-    v[1] = fmaxf(v[1], -q.x);
-    v[2] = fmaxf(v[2], -q.y);
-    v[3] = fmaxf(v[3], -q.z);
-    v[4] = fmaxf(v[4], q.x);
-    v[5] = fmaxf(v[5], q.y);
-    v[6] = fmaxf(v[6], q.z);
+    v[1] = fmaxf(v[1], -p.x);
+    v[2] = fmaxf(v[2], -p.y);
+    v[3] = fmaxf(v[3], -p.z);
+    v[4] = fmaxf(v[4], p.x);
+    v[5] = fmaxf(v[5], p.y);
+    v[6] = fmaxf(v[6], p.z);
   }
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
@@ -962,7 +958,8 @@ __global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float* __restri
   __shared__ float s_v[7][32];
   const SysDev S = sys[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float v[7] = {0.0f, 0.0f, 0.0f, 0.0f, S.box, S.box, S.box};
+  const float lowest = -3.0e38f;
+  float v[7] = {0.0f, lowest, lowest, lowest, lowest, lowest, lowest};
   for (int i = tid; i < S.n_rep; i += blockDim.x)
 #pragma unroll
     for (int k = 0; k < 7; ++k) v[k] = fmaxf(v[k], part[(size_t)(S.inst0 + i) * 8 + k]);
@@ -978,9 +975,10 @@ __global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float* __restri
       w[k] = s_v[k][0];
       for (int q = 1; q < (int)(blockDim.x >> 5); ++q) w[k] = fmaxf(w[k], s_v[k][q]);
     }
-    const float R2 = 2.02f * sqrtf(w[0]), lim = 1.49f * S.box;
-    const bool ok = (w[4] + w[1]) + R2 <= lim && (w[5] + w[2]) + R2 <= lim &&
-                    (w[6] + w[3]) + R2 <= lim;
+    const float R = 1.01f * sqrtf(w[0]), lim = 1.49f * S.box;
+    bool ok = true;
+    for (int a = 0; a < 3; ++a)  // max(p_max, L + R) - min(p_min, -R)
+      ok = ok && fmaxf(w[4 + a], S.box + R) + fmaxf(w[1 + a], R) <= lim;
     sys[blockIdx.x].fold_mi = ok ? 1 : 0;
   }
 }
@@ -2546,8 +2544,8 @@ int remc_upload_state(remc_handle* h, const float* pos, const float* rel, const 
   state_pack_kernel<<<grid, 256, 0, h->stream>>>(sp, sr, sc, h->d_bead_info, (long long)nb,
                                                  (long long)nm, h->d_pos, h->d_rel, h->d_centre);
   REMC_CUDA_TRY(cudaGetLastError());
-  fold_part_kernel<<<h->n_inst, 256, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_rel,
-                                                     h->d_centre, h->d_fold_part);
+  fold_part_kernel<<<h->n_inst, 256, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos,
+                                                     h->d_rel, h->d_fold_part);
   REMC_CUDA_TRY(cudaGetLastError());
   fold_flag_kernel<<<h->n_sys, 256, 0, h->stream>>>(h->d_sys, h->d_fold_part);
   REMC_CUDA_TRY(cudaGetLastError());

@@ -11,11 +11,11 @@ pytestmark = pytest.mark.gpu
 
 def _host_flag(s, state=None):
     pos, rel, cen, quat = s.state() if state is None else state
-    L = np.float32(s.box)
-    R = np.sqrt((rel.astype(np.float64) ** 2).sum(axis=1)).max() if len(rel) else 0.0
-    lo = np.minimum(cen.min(axis=0), 0.0)
-    hi = np.maximum(cen.max(axis=0), float(L))
-    margin = 1.49 * float(L) - ((hi - lo) + 2.02 * R)
+    L = float(np.float32(s.box))
+    R = 1.01 * np.sqrt((rel.astype(np.float64) ** 2).sum(axis=1)).max()
+    lo = np.minimum(pos.min(axis=0), -R)
+    hi = np.maximum(pos.max(axis=0), L + R)
+    margin = 1.49 * L - (hi - lo)
     return int(np.all(margin >= 0)), float(np.min(np.abs(margin)))
 
 
