@@ -509,23 +509,23 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           int j = gtid;
           // folded minimum image where the system allows it (fold_mi)
           auto pass1 = [&](auto fold) {
-          constexpr bool F = decltype(fold)::value;
-          for (; j + gstride < N; j += 2 * gstride) {
-            const int j2 = j + gstride;
-            const float4 pa = s_beads[j], pb = s_beads[j2];
-            const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
-            const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trow[bead_type(pb.w)];
-            const float2 xj = make_float2(pa.x, pb.x), yj = make_float2(pa.y, pb.y),
-                         zj = make_float2(pa.z, pb.z);
-            const float2 A2 = make_float2(Ta.x, Tb.x), C2 = make_float2(Ta.z, Tb.z);
-            const float2 en =
-                crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nnx, nny, nnz, PB1), A2, C2);
-            const float2 eo =
-                crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nox, noy, noz, PB1), A2, C2);
-            const float2 d = __fadd2_rn(en, make_float2(-eo.x, -eo.y));
-            if (j != m0) acc_o += d.x;
-            if (j2 != m0) acc_o += d.y;
-          }
+            constexpr bool F = decltype(fold)::value;
+            for (; j + gstride < N; j += 2 * gstride) {
+              const int j2 = j + gstride;
+              const float4 pa = s_beads[j], pb = s_beads[j2];
+              const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
+              const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trow[bead_type(pb.w)];
+              const float2 xj = make_float2(pa.x, pb.x), yj = make_float2(pa.y, pb.y),
+                           zj = make_float2(pa.z, pb.z);
+              const float2 A2 = make_float2(Ta.x, Tb.x), C2 = make_float2(Ta.z, Tb.z);
+              const float2 en =
+                  crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nnx, nny, nnz, PB1), A2, C2);
+              const float2 eo =
+                  crowd_energy2<R12, CUT>(pair_r2_2<F>(xj, yj, zj, nox, noy, noz, PB1), A2, C2);
+              const float2 d = __fadd2_rn(en, make_float2(-eo.x, -eo.y));
+              if (j != m0) acc_o += d.x;
+              if (j2 != m0) acc_o += d.y;
+            }
           };
           if (S.fold_mi) pass1(std::true_type{}); else pass1(std::false_type{});
           if (j < N && j != m0) {
@@ -577,31 +577,31 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             // two lanes of packed FP32
             const PackedBox PB = packed_box(box, invbox);
             auto pass2 = [&](auto fold) {
-            constexpr bool F = decltype(fold)::value;
-            for (; j + gstride < cb; j += 2 * gstride) {
-              const float4 pa = s_beads[j], pb = s_beads[j + gstride];
-              const int ta = bead_type(pa.w), tb = bead_type(pb.w);
-              const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
-                           naz = make_float2(-pa.z, -pa.z);
-              const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
-                           nbz = make_float2(-pb.z, -pb.z);
-              float a = 0.0f, c = 0.0f;
-              for (int k = 0; k < n; ++k) {
-                const float4 po = oldp[k], pn = newp[k];
-                const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
-                             kz = make_float2(pn.z, po.z);
-                const float4* row = s_tab + bead_type(po.w) * kNT;
-                const float4 Ta = row[ta], Tb = row[tb];
-                const float2 ea =
-                    kh_energy2(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
-                const float2 eb =
-                    kh_energy2(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PB), Tb, A.K.c_xi);
-                a += ea.x - ea.y;
-                c += eb.x - eb.y;
+              constexpr bool F = decltype(fold)::value;
+              for (; j + gstride < cb; j += 2 * gstride) {
+                const float4 pa = s_beads[j], pb = s_beads[j + gstride];
+                const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+                const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
+                             naz = make_float2(-pa.z, -pa.z);
+                const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
+                             nbz = make_float2(-pb.z, -pb.z);
+                float a = 0.0f, c = 0.0f;
+                for (int k = 0; k < n; ++k) {
+                  const float4 po = oldp[k], pn = newp[k];
+                  const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
+                               kz = make_float2(pn.z, po.z);
+                  const float4* row = s_tab + bead_type(po.w) * kNT;
+                  const float4 Ta = row[ta], Tb = row[tb];
+                  const float2 ea =
+                      kh_energy2(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
+                  const float2 eb =
+                      kh_energy2(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PB), Tb, A.K.c_xi);
+                  a += ea.x - ea.y;
+                  c += eb.x - eb.y;
+                }
+                acc_c += a;
+                acc_c += c;
               }
-              acc_c += a;
-              acc_c += c;
-            }
             };
             if (S.fold_mi) pass2(std::true_type{}); else pass2(std::false_type{});
           }
@@ -632,34 +632,34 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           const bool one_ct = ctype >= 0;
           const PackedBox PBc = packed_box(box, invbox);
           auto pass3 = [&](auto fold) {
-          constexpr bool F = decltype(fold)::value;
-          for (; j + gstride < hi; j += 2 * gstride) {
-            const float4 pa = s_beads[j], pb = s_beads[j + gstride];
-            const int ta = bead_type(pa.w), tb = bead_type(pb.w);
-            const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
-                         naz = make_float2(-pa.z, -pa.z);
-            const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
-                         nbz = make_float2(-pb.z, -pb.z);
-            float a = 0.0f, c = 0.0f;
-            for (int k = 0; k < n; ++k) {
-              const float4 po = oldp[k], pn = newp[k];
-              const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
-                           kz = make_float2(pn.z, po.z);
-              const float4* row = s_tab + bead_type(po.w) * kNT;
-              const float4 Ta = row[ta];
-              const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
-              const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PBc),
-                                                        make_float2(Ta.x, Ta.x),
-                                                        make_float2(Ta.z, Ta.z));
-              const float2 eb = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PBc),
-                                                        make_float2(Tb.x, Tb.x),
-                                                        make_float2(Tb.z, Tb.z));
-              a += ea.x - ea.y;
-              c += eb.x - eb.y;
+            constexpr bool F = decltype(fold)::value;
+            for (; j + gstride < hi; j += 2 * gstride) {
+              const float4 pa = s_beads[j], pb = s_beads[j + gstride];
+              const int ta = bead_type(pa.w), tb = bead_type(pb.w);
+              const float2 nax = make_float2(-pa.x, -pa.x), nay = make_float2(-pa.y, -pa.y),
+                           naz = make_float2(-pa.z, -pa.z);
+              const float2 nbx = make_float2(-pb.x, -pb.x), nby = make_float2(-pb.y, -pb.y),
+                           nbz = make_float2(-pb.z, -pb.z);
+              float a = 0.0f, c = 0.0f;
+              for (int k = 0; k < n; ++k) {
+                const float4 po = oldp[k], pn = newp[k];
+                const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
+                             kz = make_float2(pn.z, po.z);
+                const float4* row = s_tab + bead_type(po.w) * kNT;
+                const float4 Ta = row[ta];
+                const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
+                const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PBc),
+                                                          make_float2(Ta.x, Ta.x),
+                                                          make_float2(Ta.z, Ta.z));
+                const float2 eb = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nbx, nby, nbz, PBc),
+                                                          make_float2(Tb.x, Tb.x),
+                                                          make_float2(Tb.z, Tb.z));
+                a += ea.x - ea.y;
+                c += eb.x - eb.y;
+              }
+              acc_o += a;
+              acc_o += c;
             }
-            acc_o += a;
-            acc_o += c;
-          }
           };
           if (S.fold_mi) pass3(std::true_type{}); else pass3(std::false_type{});
           for (; j < hi; j += gstride) {
