@@ -4,7 +4,7 @@
 // (simulation engine/src/{Replica,Molecule,AminoAcids,AminoAcid,vector3f,
 // Quaternion,Residue,TorsionalLookupMatrix,Link}.cpp) by oracle/Makefile into
 // oracle/_ref/libremcref.so. Only tests, smoke() and bench.py's CPU baseline
-// load it, as a checker. The product never links it.
+// load it, to check the engine's results. The product never links it.
 //
 // It exposes a plain C ABI so the Python tests can:
 //   * build a reference `Replica` from flat arrays (same state the GPU engine

@@ -1,6 +1,6 @@
 /* FP64 CPU oracle for the REMC docking hot path (TEST INFRASTRUCTURE ONLY:
  * imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
- * leg as the checker; the product never links it). See remc_oracle.h for the
+ * leg to check the engine's results; the product never links it). See remc_oracle.h for the
  * reference files each function follows.
  *
  * Build: cc -O2 -fPIC -shared (default x86-64 target: no FMA contraction, so

@@ -1,7 +1,7 @@
 /* FP64 CPU oracle for the REMC docking hot path (TEST INFRASTRUCTURE).
  *
  * A plain-C restatement of the reference algorithm, used only by tests/,
- * __graft_entry__.smoke() and bench.py's cpu_baseline leg, as the checker.
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg, to check the engine's results.
  * The product library never links it.
  *
  * Reference files followed (paths inside iantunbridge/RemcDockingSimulator):

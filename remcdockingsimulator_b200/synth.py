@@ -214,7 +214,7 @@ def place_crowders(rng: np.random.Generator, n: int, radius: float, box: float,
     return crowders
 
 
-def baseline_params():
+def benchmark_params():
     # lambda = 0.16, Debye 10 A, r^-12 crowder walls with sigma = rho_i + rho_j, no cutoff
     return make_params(lambda_=0.16, e0=-2.27, debye_length=10.0, crowder_mode=1,
                        crowder_cutoff=0.0, crowder_eps=1.0)
@@ -226,7 +226,7 @@ def two_chain(seed: int = 0, mc_steps: int = 10_000) -> Workload:
     s = build_system(rng, table, [76, 24], 0, 0.0, 100.0)
     R = 20
     return Workload("two_chain", [s], [R], [geometric_ladder(290.0, 450.0, R)], 0.5, 0.2,
-                    baseline_params(), mc_steps, 1000,
+                    benchmark_params(), mc_steps, 1000,
                     "76+24-residue chains, 100 A box, 20 replicas 290-450 K")
 
 
@@ -236,7 +236,7 @@ def crowded(seed: int = 0, mc_steps: int = 100_000) -> Workload:
     s = build_system(rng, table, [76, 24], 400, 12.0, 200.0)
     R = 32
     return Workload("crowded", [s], [R], [geometric_ladder(290.0, 480.0, R)], 0.5, 0.2,
-                    baseline_params(), mc_steps, 1000,
+                    benchmark_params(), mc_steps, 1000,
                     "76+24 chains + 400 crowders R=12 A, 200 A box, 32 replicas 290-480 K")
 
 
@@ -256,7 +256,7 @@ def batch64(seed: int = 0, n_systems: int = 64, mc_steps: int = 10_000) -> Workl
         box = max((vol / phi) ** (1.0 / 3.0), 80.0)
         systems.append(build_system(rng, table, lengths, n_crowd, crowder_radius, box))
         ladders.append(geometric_ladder(290.0, 450.0, R))
-    return Workload("batch64", systems, [R] * n_systems, ladders, 0.5, 0.2, baseline_params(),
+    return Workload("batch64", systems, [R] * n_systems, ladders, 0.5, 0.2, benchmark_params(),
                     mc_steps, 1000,
                     "%d systems: 2-8 chains x 20-300 residues, 0-1000 crowders R=12 A, "
                     "packing fraction 0.1-0.3, 16 replicas" % n_systems)
@@ -270,7 +270,7 @@ def assembly(seed: int = 0, mc_steps: int = 10_000) -> Workload:
     s = build_system(rng, table, [(types, chain)] * 60, 2000, 10.0, 400.0)
     R = 32
     return Workload("assembly", [s], [R], [geometric_ladder(290.0, 500.0, R)], 0.5, 0.2,
-                    baseline_params(), mc_steps, 1000,
+                    benchmark_params(), mc_steps, 1000,
                     "60 x 150-residue chains + 2000 crowders R=10 A, 400 A box, 32 replicas")
 
 

@@ -12,7 +12,7 @@ def _system(seed):
     from remcdockingsimulator_b200 import synth
     rng = np.random.default_rng(seed)
     table = synth.contact_table(rng)
-    return synth.build_system(rng, table, [12, 9], 6, 8.0, 60.0), synth.baseline_params()
+    return synth.build_system(rng, table, [12, 9], 6, 8.0, 60.0), synth.benchmark_params()
 
 
 def test_oracle_forces_match_central_differences(oracle_built, built_lib):

@@ -89,7 +89,7 @@ def test_system_too_large_for_shared_memory(built_lib):
     from remcdockingsimulator_b200.model import geometric_ladder
     s = _large_system()
     assert s.n_beads > 15000
-    params = synth.baseline_params()
+    params = synth.benchmark_params()
     R = 2
     lad = geometric_ladder(300.0, 350.0, R)
     with Engine([s], R, params) as eng:

@@ -75,7 +75,7 @@ def test_tight_box_trajectory_vs_oracle(built_lib):
     s = _tight_box()
     R = 3
     w = synth.Workload("tight", [s], [R], [synth.geometric_ladder(300.0, 500.0, R)], 1.0, 0.2,
-                       synth.baseline_params(), 2000, 1000)
+                       synth.benchmark_params(), 2000, 1000)
     _run_sweep_vs_oracle(w, R, 2000, seed=17)
 
 

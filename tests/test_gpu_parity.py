@@ -58,7 +58,7 @@ def test_energy_full_uneven_batch_vs_oracle(built_lib):
     systems = [synth.build_system(rng, table, [int(rng.integers(20, 200)) for _ in range(k)],
                                   int(rng.integers(0, 300)), 12.0, 160.0 + 20 * k)
                for k in (2, 3, 5, 8)]
-    p = synth.baseline_params()
+    p = synth.benchmark_params()
     with _engine(systems, [3, 1, 2, 4], p) as eng:
         e = eng.energy_full()
         first = eng.inst_first
