@@ -149,34 +149,77 @@ class ClockSampler:
 PAIRS_PER_CORE_S = 2.5e7  # order of the reference E() rate per core (pairs/s)
 
 
+def inter_molecular_pairs(system) -> int:
+    """Pairs the reference's Replica::E() evaluates every MC step (all bead
+    pairs of different molecules, Replica.cpp:603-745)."""
+    n = system.n_beads
+    return (n * (n - 1) - sum(m.n * (m.n - 1) for m in system.molecules)) // 2
+
+
 def reference_sample_plan(workload, seed: int, cores: int, seconds: float):
-    """Pick up to 8 systems of the workload (seeded) and an MC step count so
-    that one sample is about `seconds` of work for `cores` threads of the
-    reference engine, which evaluates the full O(N^2) energy every step."""
-    import numpy as np
+    """Replicas of the workload for the reference engine and an MC step count
+    so that one sample is about `seconds` of work on `cores` threads (the
+    reference evaluates the full O(N^2) energy every step). Every system of
+    the workload takes part with the same number of its replicas, so the
+    sample has the workload's own mix of system sizes; a system's replicas
+    differ only in temperature, and their cost per step is the same.
+    Returns [(system index, ladder index)] and the MC step count."""
     n = len(workload.systems)
-    rng = np.random.default_rng(seed + 777)
-    k = min(n, 8)
-    systems = sorted(rng.choice(n, size=k, replace=False).tolist())
-    pairs = sum(workload.n_replicas[i] * workload.systems[i].n_beads ** 2 / 2.0 for i in systems)
+    per = max(1, min(min(workload.n_replicas), -(-2 * cores // n)))
+    picks = []
+    for si in range(n):
+        R = workload.n_replicas[si]
+        idx = sorted({int(round(k * (R - 1) / max(per - 1, 1))) for k in range(per)})
+        picks.extend((si, k) for k in idx)
+    pairs = sum(inter_molecular_pairs(workload.systems[si]) for si, _ in picks)
     mc = int(PAIRS_PER_CORE_S * cores * seconds / max(pairs, 1.0))
-    return systems, max(2, min(mc, 2000))
+    return picks, max(2, min(mc, 2000))
 
 
-def build_reference_replicas(workload, systems):
+def balanced_order(costs, threads: int):
+    """Order of the replicas such that the contiguous slices the timing
+    harness hands to its threads (main.cpp:879-883) carry near-equal work:
+    each replica, in decreasing cost, joins the least loaded slice that still
+    has room."""
+    n = len(costs)
+    threads = max(1, min(threads, n))
+    per = -(-n // threads)
+    slices = [[] for _ in range(threads)]
+    load = [0.0] * threads
+    for i in sorted(range(n), key=lambda i: -costs[i]):
+        k = min((t for t in range(threads) if len(slices[t]) < per), key=lambda t: load[t])
+        slices[k].append(i)
+        load[k] += costs[i]
+    return [i for sl in slices for i in sl]
+
+
+def build_reference_replicas(workload, picks, threads: int = 1):
     """The reference's own Replica objects (oracle/_ref, compiled from its
-    sources) for every replica of the sampled systems; the reference
-    executable itself cannot load more than 30 molecules (double free in
-    Replica::loadMolecule), so the replicas are built through the harness."""
+    sources), one per (system, ladder index) pick, in an order that balances
+    the harness's thread slices; the reference executable itself cannot load
+    more than 30 molecules (double free in Replica::loadMolecule), so the
+    replicas are built through the harness. Returns the replicas and their
+    inter-molecular pair counts."""
     from oracle import bindings as ob
-    reps = []
-    for si in systems:
+    costs = [inter_molecular_pairs(workload.systems[si]) for si, _ in picks]
+    reps, pairs = [], []
+    for i in balanced_order(costs, threads):
+        si, k = picks[i]
         s = workload.systems[si]
-        for T in workload.ladders[si]:
-            r = ob.ReferenceReplica(s, temperature=float(T))
-            r.set_steps(workload.translate_step, workload.rotate_step)
-            reps.append(r)
-    return reps
+        r = ob.ReferenceReplica(s, temperature=float(workload.ladders[si][k]))
+        r.set_steps(workload.translate_step, workload.rotate_step)
+        reps.append(r)
+        pairs.append(costs[i])
+    return reps, pairs
+
+
+def maps_engine_library() -> bool:
+    """True if this process has this repository's engine library mapped."""
+    try:
+        with open("/proc/self/maps") as fh:
+            return "libremc_b200" in fh.read()
+    except OSError:
+        return False
 
 
 def time_reference(reps, threads: int, mc: int):
@@ -417,30 +460,32 @@ def main():
 def cpu_baseline(workload, seed: int):
     cores = os.cpu_count() or 1
     try:
-        systems, mc = reference_sample_plan(workload, seed, cores, 10.0)
-        reps = build_reference_replicas(workload, systems)
-        wall = time_reference(reps, cores, mc)
+        picks, mc = reference_sample_plan(workload, seed, cores, 10.0)
+        threads = min(cores, len(picks))
+        reps, pairs = build_reference_replicas(workload, picks, threads)
+        wall = time_reference(reps, threads, mc)
         n_rs = len(reps) * mc
         # the reference's own Replica::E() on one core (its "Host Timer" figure,
         # Replica.cpp:1082): inter-molecular pairs evaluated per second
         r0 = reps[0]
-        s0 = workload.systems[systems[0]]
-        pairs = (s0.n_beads * (s0.n_beads - 1) - sum(m.n * (m.n - 1) for m in s0.molecules)) // 2
         calls, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < 1.0:
             r0.E()
             calls += 1
-        e_rate = pairs * calls / (time.perf_counter() - t0)
+        e_rate = pairs[0] * calls / (time.perf_counter() - t0)
         for r in reps:
             r.close()
-        return {"value": n_rs / wall, "unit": "replica-steps/s", "cores": min(cores, len(reps)),
+        n_sys = len({si for si, _ in picks})
+        return {"value": n_rs / wall, "unit": "replica-steps/s", "cores": threads,
+                "pair_energies_per_s": sum(pairs) * mc / wall,
                 "e_pairs_per_s_one_core": e_rate,
                 "kind": "reference",
                 "sample": "reference Replica::MCSearch (compiled from its sources, full energy "
-                          "every step, its own (6/r)^6 crowder model and lambda=0.159) on all "
-                          "%d replicas of %d of %d systems x %d MC steps, %d threads, %.1f s" %
-                          (len(reps), len(systems), len(workload.systems), mc,
-                           min(cores, len(reps)), wall)}
+                          "every step, its own (6/r)^6 crowder model and lambda=0.159) on %d "
+                          "replicas (%d of each of the %d of %d systems) x %d MC steps, %d "
+                          "threads, %.1f s" %
+                          (len(reps), len(reps) // max(n_sys, 1), n_sys,
+                           len(workload.systems), mc, threads, wall)}
     except Exception as exc:  # reported, not fatal: the GPU number stands alone
         return {"value": None, "unit": "replica-steps/s", "cores": 0, "kind": "reference",
                 "sample": "failed: %s" % str(exc)[:300]}
@@ -457,9 +502,9 @@ def reference_arm(args, world: int, rank: int):
     from remcdockingsimulator_b200 import synth
     w = synth.WORKLOADS[args.workload](args.seed)
     cores = os.cpu_count() or 1
-    systems, mc = reference_sample_plan(w, args.seed, cores, 4.0)
-    reps = build_reference_replicas(w, systems)
-    threads = min(cores, len(reps))
+    picks, mc = reference_sample_plan(w, args.seed, cores, 4.0)
+    threads = min(cores, len(picks))
+    reps, pairs = build_reference_replicas(w, picks, threads)
     for _ in range(args.warmup):
         time_reference(reps, threads, max(1, mc // 8))
     total_t = 0.0
@@ -468,6 +513,13 @@ def reference_arm(args, world: int, rank: int):
     for r in reps:
         r.close()
     value = len(reps) * mc * args.steps / total_t
+    pair_rate = sum(pairs) * mc * args.steps / total_t
+    n_sys = len({si for si, _ in picks})
+    sample = ("reference Replica::MCSearch (compiled from its sources, full energy every step, "
+              "its own (6/r)^6 crowder model and lambda=0.159) on %d replicas (%d of each of "
+              "the %d of %d systems, so the batch's own mix of sizes) x %d MC steps per bench "
+              "step, %d threads" % (len(reps), len(reps) // max(n_sys, 1), n_sys, len(w.systems),
+                                    mc, threads))
     line = {
         "impl": "reference",
         "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",
@@ -476,12 +528,13 @@ def reference_arm(args, world: int, rank: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic (seeded generator with the benchmark configuration's shapes)",
         "config": {"workload": w.name, "description": w.description,
-                   "sample_systems": systems, "mc_steps_per_sample": mc},
+                   "sample_replicas": len(reps), "sample_systems": n_sys,
+                   "mc_steps_per_sample": mc},
+        "pair_energies_per_s": pair_rate,
+        "pair_energy_note": "pairs of the full energy the reference evaluates every MC step",
+        "engine_library_mapped": maps_engine_library(),
         "cpu_baseline": {"value": value, "unit": "replica-steps/s", "cores": threads,
-                         "kind": "reference",
-                         "sample": "reference Replica::MCSearch on all %d replicas of %d of %d "
-                                   "systems x %d MC steps per bench step, %d threads" %
-                                   (len(reps), len(systems), len(w.systems), mc, threads)},
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "replica-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -22,10 +22,28 @@ def _ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+def reference_params() -> Params:
+    """The reference's compile-time energy constants (definitions.h:11-35,
+    Replica.cpp:624), built without loading the engine library: the same
+    FP32 values remc_default_params writes (a CPU test compares the two)."""
+    from .model import DH_CONSTANT, KBT_CONVERSION_FACTOR, LJ_CONVERSION_FACTOR
+    p = Params()
+    p.lambda_ = 0.159
+    p.e0 = -2.27
+    p.debye_length = 10.0
+    p.dh_const = float(DH_CONSTANT)
+    p.lj_cf = float(LJ_CONVERSION_FACTOR)
+    p.kbt_cf = float(KBT_CONVERSION_FACTOR)
+    p.crowder_mode = 0
+    p.crowder_cutoff = 15.0
+    p.crowder_eps = 1.0
+    return p
+
+
 def make_params(lambda_: float = 0.159, e0: float = -2.27, debye_length: float = 10.0,
                 crowder_mode: int = 0, crowder_cutoff: float = 15.0,
                 crowder_eps: float = 1.0) -> Params:
-    p = _capi.default_params()
+    p = reference_params()
     p.lambda_ = lambda_
     p.e0 = e0
     p.debye_length = debye_length

@@ -49,6 +49,27 @@ def test_default_params_are_reference_constants(built_lib):
     assert np.float32(p.dh_const) == model.DH_CONSTANT
     assert np.float32(p.lj_cf) == model.LJ_CONVERSION_FACTOR
     assert p.crowder_mode == 0 and np.float32(p.crowder_cutoff) == np.float32(15.0)
+    # the pure-Python copy (used where the engine library must not be loaded,
+    # e.g. the benchmark's reference arm) holds the same FP32 values
+    from remcdockingsimulator_b200.engine import reference_params
+    q = reference_params()
+    for name, _ in type(p)._fields_:
+        assert getattr(q, name) == getattr(p, name), name
+
+
+def test_workload_generation_does_not_load_the_engine_library():
+    """Building a benchmark workload (what the reference arm of bench.py does)
+    maps nothing of this repository's native code."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from remcdockingsimulator_b200 import synth\n"
+            "w = synth.two_chain(1)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libremc_b200' not in maps and 'libremc_replica' not in maps\n"
+            "print('clean')\n" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "clean" in r.stdout, r.stderr
 
 
 def test_create_rejects_bad_descriptors_without_gpu(built_lib):

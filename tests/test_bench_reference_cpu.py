@@ -34,3 +34,20 @@ def test_reference_arm_prints_one_contract_line():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    # the arm runs the reference alone: this repository's engine library is
+    # never mapped into its process
+    assert d["engine_library_mapped"] is False
+    assert d["pair_energies_per_s"] > d["value"]
+    # every system of the batch takes part (the batch's own mix of sizes)
+    assert d["config"]["sample_systems"] == 64
+
+
+def test_balanced_slices():
+    sys.path.insert(0, ROOT)
+    import bench
+    costs = [100, 1, 50, 50, 3, 90, 10, 10, 20, 60, 5, 5]
+    order = bench.balanced_order(costs, 4)
+    assert sorted(order) == list(range(len(costs)))
+    per = 3
+    loads = [sum(costs[i] for i in order[k * per:(k + 1) * per]) for k in range(4)]
+    assert max(loads) - min(loads) <= 40, loads
