@@ -53,7 +53,9 @@ void CUDA_translateMolecule(float4* d_residuePositions, int* d_startPosition,
 
 /* cudaExterns.h:23 - full-system energy into *result (host), synchronous.
  * residueCount, moleculePositions, moleculeCount, blockSize and
- * sharedMemSize are accepted for compatibility; datasetSize beads are read. */
+ * sharedMemSize are accepted for compatibility; datasetSize beads are read.
+ * Runs on the legacy default stream. Safe to call from several host threads
+ * at once: the calls take turns on their shared partial-sum buffer. */
 void CUDA_EonDevice(float4* residuePositions, float4* residueMeta, int* residueCount,
                     int* moleculePositions, int* moleculeCount, float* LJPotentials,
                     double* result, int blockSize, int datasetSize, int sharedMemSize);
@@ -70,7 +72,11 @@ int CUDA_memcpy_to_host_async(void* destination, void* source, int mem_size,
  * block in device_result (resultSize x resultSize) for the host to sum and
  * scale by KBTConversionFactor (Replica::SumGridResults, Replica.cpp:1195-1216);
  * here device_result[0] holds the whole sum in those units and the other
- * entries are zero, so the same host summation gives the energy. */
+ * entries are zero, so the same host summation gives the energy.
+ * Each (device, stream) has its own partial-sum buffer, kept until exit and
+ * grown only after the stream's queued work has finished: energies queued on
+ * different streams (the reference gives every replica thread its own,
+ * main.cpp:924-954) may run concurrently, from any host threads. */
 void CUDA_EonDevice_async(float4* residuePositions, float4* residueMeta, int* residueCount,
                           int* moleculePositions, int* moleculeCount, float* LJPotentials,
                           float* device_result, int resultSize, int blockSize, int datasetSize,
@@ -116,6 +122,10 @@ void unbindLJTexture(void);
 int CUDA_EonDevice_noalloc(const float4* residuePositions, const float4* residueMeta,
                            const float* LJPotentials, int datasetSize, double* d_result,
                            cudaStream_t stream);
+
+/* The device buffers and addresses the calls above keep per device are not
+ * renewed after cudaDeviceReset: do not reset a device while this library
+ * uses it. */
 
 /* Energy-model constants used by the calls above (default: the reference's
  * compile-time values, remc_default_params). No reference counterpart. */

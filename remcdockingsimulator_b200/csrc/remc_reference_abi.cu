@@ -15,8 +15,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "../../include/remc_reference_abi.h"
 #include "remc_device.cuh"
@@ -42,8 +45,19 @@ float g_box = 150.0f;  // BOUNDING_VALUE until CUDA_setBoxDimension (definitions
 float* g_bound_table = nullptr;
 bool g_params_set = false;
 remc_params g_params;
-double* g_scratch[kMaxDevices] = {nullptr};
-size_t g_scratch_cap[kMaxDevices] = {0};
+
+// Scratch for the per-item partials of the allocating energy calls, one
+// buffer per (device, stream). A call holds its buffer's lock from the
+// lookup until its last launch (and, on the synchronous path, its result
+// copy) is enqueued, so calls on one stream take their turns in stream order,
+// and calls on different streams or host threads never share partials.
+struct ScratchSlot {
+  std::mutex mu;
+  double* ptr = nullptr;
+  size_t cap = 0;
+};
+std::mutex g_slots_mutex;
+std::map<std::pair<int, cudaStream_t>, std::unique_ptr<ScratchSlot>> g_slots;
 
 void set_status(int code, const char* what, cudaError_t e = cudaSuccess) {
   g_status = code;
@@ -55,12 +69,13 @@ void set_status(int code, const char* what, cudaError_t e = cudaSuccess) {
   }
 }
 
-RefConsts make_consts() {
+RefConsts make_consts(float* unscale = nullptr) {
   std::lock_guard<std::mutex> lock(g_mutex);
   if (!g_params_set) {
     remc_default_params(&g_params);
     g_params_set = true;
   }
+  if (unscale) *unscale = 1.0f / (float)((double)g_params.kbt_cf);
   RefConsts C;
   C.lambda_ = g_params.lambda_;
   C.e0 = g_params.e0;
@@ -209,24 +224,36 @@ __global__ void translate_center_kernel(float4* center, const float4* t) {
   center->z += v.z;
 }
 
-// Scratch for the per-item partials, grown per device (never per call once
-// large enough). Returns null on failure.
-double* device_scratch(size_t n) {
+// The scratch buffer of (current device, stream), locked by `lock`, holding
+// at least n doubles. Growing it first waits for the work already queued on
+// the stream (the only work that can still read the old buffer) and frees it.
+// Returns null on failure.
+double* stream_scratch(cudaStream_t stream, size_t n, std::unique_lock<std::mutex>& lock) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  std::lock_guard<std::mutex> lock(g_mutex);
-  if (g_scratch_cap[dev] < n) {
-    if (g_scratch[dev]) {
-      cudaDeviceSynchronize();
-      cudaFree(g_scratch[dev]);
-      g_scratch[dev] = nullptr;
-      g_scratch_cap[dev] = 0;
-    }
-    size_t cap = std::max<size_t>(n, 4096);
-    if (cudaMalloc(&g_scratch[dev], cap * sizeof(double)) != cudaSuccess) return nullptr;
-    g_scratch_cap[dev] = cap;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return nullptr;
+  ScratchSlot* slot;
+  {
+    std::lock_guard<std::mutex> g(g_slots_mutex);
+    std::unique_ptr<ScratchSlot>& p = g_slots[std::make_pair(dev, stream)];
+    if (!p) p.reset(new ScratchSlot());
+    slot = p.get();
   }
-  return g_scratch[dev];
+  lock = std::unique_lock<std::mutex>(slot->mu);
+  if (slot->cap < n) {
+    if (slot->ptr) {
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return nullptr;
+      cudaFree(slot->ptr);
+      slot->ptr = nullptr;
+      slot->cap = 0;
+    }
+    const size_t cap = std::max<size_t>(n, 4096);
+    if (cudaMalloc(&slot->ptr, cap * sizeof(double)) != cudaSuccess) {
+      slot->ptr = nullptr;
+      return nullptr;
+    }
+    slot->cap = cap;
+  }
+  return slot->ptr;
 }
 
 // ---- allocation-free energy (CUDA_EonDevice_noalloc)
@@ -263,7 +290,8 @@ int enqueue_energy(const float4* pos, const float4* meta, const float* table, in
                    double* scratch, float* grid_out, int grid_n, cudaStream_t stream) {
   const int T = (P + kRefTile - 1) / kRefTile;
   const int n = T * (T + 1) / 2;
-  const RefConsts C = make_consts();
+  float unscale = 1.0f;
+  const RefConsts C = make_consts(&unscale);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -274,8 +302,7 @@ int enqueue_energy(const float4* pos, const float4* meta, const float* table, in
     set_status(REMC_ERR_CUDA, "energy kernel launch", e);
     return REMC_ERR_CUDA;
   }
-  ref_energy_sum<<<1, 256, 0, stream>>>(scratch, n, scratch + n, grid_out, grid_n,
-                                        1.0f / (float)((double)g_params.kbt_cf));
+  ref_energy_sum<<<1, 256, 0, stream>>>(scratch, n, scratch + n, grid_out, grid_n, unscale);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_status(REMC_ERR_CUDA, "energy sum launch", e);
@@ -377,12 +404,15 @@ void CUDA_EonDevice(float4* pos, float4* meta, int* residueCount, int* moleculeP
   if (!energy_args_ok(pos, meta, table, datasetSize)) return;
   const int T = (datasetSize + kRefTile - 1) / kRefTile;
   const size_t n = (size_t)T * (T + 1) / 2;
-  double* scratch = device_scratch(n + 1);
+  // the reference's synchronous path runs on the legacy default stream; the
+  // result copy is made under the scratch lock, before another host thread
+  // can queue its energy on the same buffer
+  std::unique_lock<std::mutex> lock;
+  double* scratch = stream_scratch(0, n + 1, lock);
   if (!scratch) {
     set_status(REMC_ERR_NOMEM, "scratch allocation failed");
     return;
   }
-  // the reference's synchronous path runs on the legacy default stream
   if (enqueue_energy(pos, meta, table, datasetSize, scratch, nullptr, 0, 0) != REMC_OK) return;
   cudaError_t e = cudaMemcpy(result, scratch + n, sizeof(double), cudaMemcpyDeviceToHost);
   set_status(e == cudaSuccess ? REMC_OK : REMC_ERR_CUDA, "result copy", e);
@@ -405,7 +435,11 @@ void CUDA_EonDevice_async(float4* pos, float4* meta, int* residueCount, int* mol
   if (!energy_args_ok(pos, meta, table, datasetSize)) return;
   const int T = (datasetSize + kRefTile - 1) / kRefTile;
   const size_t n = (size_t)T * (T + 1) / 2;
-  double* scratch = device_scratch(n + 1);
+  // the stream's own scratch: energies queued on other streams run
+  // concurrently on other buffers, and the next call on this stream reuses
+  // this one only after this call's kernels, in stream order
+  std::unique_lock<std::mutex> lock;
+  double* scratch = stream_scratch(stream, n + 1, lock);
   if (!scratch) {
     set_status(REMC_ERR_NOMEM, "scratch allocation failed");
     return;

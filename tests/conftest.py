@@ -38,6 +38,29 @@ def golden_system(golden, table, k):
     return System(mols, golden["box"], table)
 
 
+def crowder_lattice(n, spacing=8.0, seed=5, side=None):
+    """n one-bead crowders on a jittered cubic lattice of `side` sites per
+    edge (spacing 8 A, inside the 15 A cutoff of the reference's (6/r)^6
+    crowder term), in a box of side * spacing."""
+    from remcdockingsimulator_b200 import synth
+    from remcdockingsimulator_b200.model import CROWDER_TYPE, Molecule, System
+    rng = np.random.default_rng(seed)
+    side = side or int(np.ceil(n ** (1.0 / 3.0)))
+    assert side ** 3 >= n
+    box = side * spacing
+    g = np.stack(np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij"),
+                 axis=-1).reshape(-1, 3)[:n]
+    xyz = g * spacing + 1.0 + rng.uniform(-0.4, 0.4, size=(n, 3))  # inside [0, box)
+    mols = []
+    for c in xyz:
+        m = Molecule.from_beads([CROWDER_TYPE], np.zeros((1, 3), np.float32))
+        m.crowder = True
+        m.set_position(c.astype(np.float32))
+        mols.append(m)
+    table = synth.contact_table(np.random.default_rng(seed))
+    return System(mols, float(np.float32(box)), table, crowder_radius=3.0)
+
+
 @pytest.fixture(scope="session")
 def built_lib():
     from remcdockingsimulator_b200 import build

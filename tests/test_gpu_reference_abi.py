@@ -143,3 +143,76 @@ def test_translate_and_rotate_molecule(built_lib):
     off = before - c_now[:3]
     exp = np.stack([-off[:, 0], -off[:, 1], off[:, 2]], axis=1) + c_now[:3]
     assert np.allclose(after, exp, atol=1e-3)
+
+
+def test_eondevice_concurrent_streams_and_threads(built_lib):
+    """Energies of two different systems queued at the same time from two host
+    threads, on two streams (CUDA_EonDevice_async) and on the default stream
+    (CUDA_EonDevice), equal the energies of the same calls made one at a
+    time: every stream has its own partial sums, and synchronous calls take
+    turns on theirs."""
+    import threading
+    import torch
+    from conftest import crowder_lattice
+    from remcdockingsimulator_b200.reference_abi import abi, pack_reference_layout
+    L = abi()
+    systems = [crowder_lattice(16000, seed=11, side=26), crowder_lattice(12000, seed=12, side=26)]
+    assert systems[0].box == systems[1].box  # the box is one process-wide setting
+    L.CUDA_setBoxDimension(systems[0].box)
+    dev = []
+    for s in systems:
+        pos, meta = pack_reference_layout(s, 32)
+        table = np.ascontiguousarray(s.table.pairs, np.float32).reshape(-1)
+        dev.append((_dev(pos), _dev(meta), _dev(table), pos.shape[0]))
+
+    def sync_energy(k):
+        dp, dm, dt, n = dev[k]
+        out = C.c_double(0.0)
+        L.CUDA_EonDevice(C.c_void_p(dp.data_ptr()), C.c_void_p(dm.data_ptr()), None, None, None,
+                         C.c_void_p(dt.data_ptr()), C.byref(out), 32, n, 0)
+        assert L.remc_reference_abi_status() == 0
+        return out.value
+
+    def async_energy(k, stream, res):
+        dp, dm, dt, n = dev[k]
+        L.CUDA_EonDevice_async(C.c_void_p(dp.data_ptr()), C.c_void_p(dm.data_ptr()), None, None,
+                               None, C.c_void_p(dt.data_ptr()), C.c_void_p(res.data_ptr()), 1, 32,
+                               n, 0, C.c_void_p(stream.cuda_stream))
+        assert L.remc_reference_abi_status() == 0
+
+    alone_sync = [sync_energy(0), sync_energy(1)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    alone_async = []
+    for k in range(2):
+        r = torch.zeros(1, dtype=torch.float32, device="cuda")
+        async_energy(k, streams[k], r)
+        streams[k].synchronize()
+        alone_async.append(float(r.item()))
+    assert alone_async[0] != alone_async[1]
+
+    reps = 24
+    got_async = [[torch.zeros(1, dtype=torch.float32, device="cuda") for _ in range(reps)]
+                 for _ in range(2)]
+    got_sync = [[None] * reps for _ in range(2)]
+    errors = []
+
+    def worker(k):
+        try:
+            torch.cuda.set_device(0)
+            for i in range(reps):
+                async_energy(k, streams[k], got_async[k][i])
+                got_sync[k][i] = sync_energy(k)
+        except Exception as exc:  # reported below
+            errors.append(exc)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    torch.cuda.synchronize()
+    assert not errors, errors
+    for k in range(2):
+        assert all(v == alone_sync[k] for v in got_sync[k]), (k, got_sync[k], alone_sync[k])
+        vals = [float(r.item()) for r in got_async[k]]
+        assert all(v == alone_async[k] for v in vals), (k, vals, alone_async[k])
