@@ -7,10 +7,17 @@ Produces:
                                      tree) + ref_harness.cpp
   oracle/_ref/REMCDockingCPU       - the reference CPU executable, same sources
                                      + its main.cpp
+  oracle/_ref/REMCDockingGPU       - the reference's own GPU build (-DEnableCUDA),
+  oracle/_ref/REMCDockingGPU_streams  and its stream build (-DEnableStreams),
+                                     from the same unmodified sources, with
+                                     include/remc_cudaexterns.h force-included
+                                     in place of its cudaExterns.h and linked
+                                     against this repository's libremc_b200.so
+                                     instead of its CudaFunctions.cu
 
-The reference tree is read where it lies (default
-/root/reference/simulation engine/src, override with REMC_REFERENCE_SRC);
-nothing is copied into this repository. Missing GSL / cutil headers are
+The reference tree is read where it lies: the directory REMC_REFERENCE_ROOT
+names, by default a directory `reference` beside this repository's root, and
+its `simulation engine/src`; nothing is copied into this repository. Missing GSL / cutil headers are
 replaced by the project-written stubs in oracle/ref_stubs/. When the tree is
 absent (e.g. on a machine that only received the prebuilt files) the
 reference build is skipped and the prebuilt files are used as they are.
@@ -27,7 +34,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
 STUBS = os.path.join(HERE, "ref_stubs")
-DEFAULT_REF_SRC = "/root/reference/simulation engine/src"
 REF_UNITS = ["AminoAcid", "AminoAcids", "Link", "Molecule", "Quaternion", "Replica", "Residue",
              "TorsionalLookupMatrix", "vector3f"]
 # the reference's own CPU flags (simulation engine/Makefile:17); gnu++11 only
@@ -59,8 +65,16 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
+def reference_root() -> str:
+    """Root of the reference project: $REMC_REFERENCE_ROOT, else `reference`
+    beside this repository's root."""
+    repo = os.path.dirname(HERE)
+    return os.environ.get("REMC_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(repo), "reference"))
+
+
 def reference_src() -> str:
-    return os.environ.get("REMC_REFERENCE_SRC", DEFAULT_REF_SRC)
+    return os.path.join(reference_root(), "simulation engine", "src")
 
 
 def build_reference(force: bool = False) -> bool:
@@ -98,10 +112,52 @@ def build_reference(force: bool = False) -> bool:
     return True
 
 
+def build_reference_gpu(force: bool = False) -> bool:
+    """The reference's own GPU executables, linked against libremc_b200.so:
+    every unit of the reference compiled unmodified with -DEnableCUDA (and
+    -DEnableStreams for the stream build), with include/remc_cudaexterns.h
+    force-included so that its `#include "cudaExterns.h"` resolves to this
+    library's entry points. Needs the engine library built first. Returns
+    False when the reference tree or the library is absent."""
+    src_dir = reference_src()
+    repo = os.path.dirname(HERE)
+    libdir = os.path.join(repo, "remcdockingsimulator_b200", "lib")
+    lib = os.path.join(libdir, "libremc_b200.so")
+    if not os.path.isdir(src_dir) or not os.path.exists(lib):
+        return False
+    shim = os.path.join(repo, "include", "remc_cudaexterns.h")
+    inc = ["-I" + STUBS, "-I" + src_dir, "-I" + os.path.join(repo, "include"),
+           "-I/usr/local/cuda/include", "-include", shim]
+    deps = ([shim, os.path.join(repo, "include", "remc_reference_abi.h")] +
+            [os.path.join(dp, f) for dp, _, fs in os.walk(STUBS) for f in fs])
+    for name, defs in (("REMCDockingGPU", ["-DEnableCUDA"]),
+                       ("REMCDockingGPU_streams", ["-DEnableCUDA", "-DEnableStreams"])):
+        objdir = os.path.join(REF_OUT, "obj_" + name)
+        os.makedirs(objdir, exist_ok=True)
+        objs = []
+        for unit in REF_UNITS + ["main"]:
+            s = os.path.join(src_dir, unit + ".cpp")
+            o = os.path.join(objdir, unit + ".o")
+            if force or _stale(o, [s] + deps):
+                _run(["g++"] + REF_CFLAGS + defs + inc + ["-c", s, "-o", o])
+            objs.append(o)
+        exe = os.path.join(REF_OUT, name)
+        if force or _stale(exe, objs + [lib]):
+            # the library is found next to the repository at run time
+            _run(["g++", "-o", exe] + objs +
+                 ["-pthread", "-L" + libdir, "-lremc_b200", "-L/usr/local/cuda/lib64", "-lcudart",
+                  "-L/usr/local/cuda/lib64/stubs", "-lcuda",
+                  "-Wl,-rpath,$ORIGIN/../../remcdockingsimulator_b200/lib",
+                  "-Wl,-rpath,/usr/local/cuda/lib64"])
+    return True
+
+
 def main() -> int:
     force = "--force" in sys.argv
     print("oracle:", build_oracle(force))
     print("reference:", "built" if build_reference(force) else "tree absent, skipped")
+    print("reference GPU build:",
+          "built" if build_reference_gpu(force) else "tree or engine library absent, skipped")
     return 0
 
 

@@ -2,7 +2,7 @@
 //
 // This file is compiled together with the UNMODIFIED reference sources
 // (simulation engine/src/{Replica,Molecule,AminoAcids,AminoAcid,vector3f,
-// Quaternion,Residue,TorsionalLookupMatrix,Link}.cpp) by oracle/Makefile into
+// Quaternion,Residue,TorsionalLookupMatrix,Link}.cpp) by oracle/build.py into
 // oracle/_ref/libremcref.so. Only tests, smoke() and bench.py's CPU baseline
 // load it, to check the engine's results. The product never links it.
 //

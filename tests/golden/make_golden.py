@@ -35,7 +35,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-REF = os.environ.get("REMC_REFERENCE_ROOT", "/root/reference")
+from oracle.build import reference_root  # noqa: E402
+
+REF = reference_root()
 SE = os.path.join(REF, "simulation engine")
 PP = os.path.join(REF, "post processor")
 BOX = 118.4

@@ -71,10 +71,12 @@ def test_golden_structure_shapes(golden):
 
 
 # ---------------------------------------------------------------- reference engine
+from oracle.build import reference_src  # noqa: E402
+
 ref_needed = pytest.mark.skipif(
     not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref",
                                     "libremcref.so")) and
-    not os.path.isdir("/root/reference/simulation engine/src"),
+    not os.path.isdir(reference_src()),
     reason="reference harness not built here")
 
 
