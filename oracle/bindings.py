@@ -69,6 +69,9 @@ def oracle_lib():
         L.oracle_energy_molecule.argtypes = [C.POINTER(OracleSystem), C.POINTER(OracleParams),
                                              PF, C.c_int, PF]
         L.oracle_energy_molecule.restype = C.c_double
+        L.oracle_energy_molecule_abs.argtypes = [C.POINTER(OracleSystem), C.POINTER(OracleParams),
+                                                 PF, C.c_int, PF]
+        L.oracle_energy_molecule_abs.restype = C.c_double
         L.oracle_noncrowder_pair_energy.argtypes = [C.POINTER(OracleSystem),
                                                     C.POINTER(OracleParams), PF]
         L.oracle_noncrowder_pair_energy.restype = C.c_double
@@ -185,6 +188,13 @@ class FP64Oracle:
         mpos = np.ascontiguousarray(mpos, np.float32)
         return oracle_lib().oracle_energy_molecule(C.byref(self.s), C.byref(self.params),
                                                    _p(pos, C.c_float), m, _p(mpos, C.c_float))
+
+    def energy_molecule_abs(self, pos: np.ndarray, m: int, mpos: np.ndarray) -> float:
+        """Sum of |pair term| of molecule m placed at mpos against the rest."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        mpos = np.ascontiguousarray(mpos, np.float32)
+        return oracle_lib().oracle_energy_molecule_abs(C.byref(self.s), C.byref(self.params),
+                                                       _p(pos, C.c_float), m, _p(mpos, C.c_float))
 
     def noncrowder_pair_energy(self, pos: np.ndarray) -> float:
         pos = np.ascontiguousarray(pos, np.float32)

@@ -182,6 +182,29 @@ double oracle_energy_molecule(const oracle_system* s, const oracle_params* p, co
   return combine(p, lj_acc, dh_acc);
 }
 
+/* Sum of the magnitudes of the pair terms of molecule m at positions mpos
+ * against every other molecule: the scale of the cancellation in a move's
+ * dE (the sum of these terms at the new and at the old position). */
+double oracle_energy_molecule_abs(const oracle_system* s, const oracle_params* p,
+                                  const float* pos, int m, const float* mpos) {
+  double acc = 0.0;
+  int m0 = s->mol_start[m], m1 = s->mol_start[m + 1];
+  for (int mj = 0; mj < s->n_mol; ++mj) {
+    if (mj == m) continue;
+    int crowd = (s->mol_role[m] == -1) || (s->mol_role[mj] == -1);
+    for (int a = m0; a < m1; ++a) {
+      for (int b = s->mol_start[mj]; b < s->mol_start[mj + 1]; ++b) {
+        double d[3];
+        double r = min_image_r(mpos + 3 * (a - m0), pos + 3 * b, (double)s->box, d);
+        double lj, dh;
+        pair_terms(s, p, s->bead_type[a], s->bead_type[b], crowd, r, &lj, &dh);
+        acc += fabs(combine(p, lj, dh));
+      }
+    }
+  }
+  return acc;
+}
+
 double oracle_noncrowder_pair_energy(const oracle_system* s, const oracle_params* p,
                                      const float* pos) {
   double total = 0.0;

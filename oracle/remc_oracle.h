@@ -83,6 +83,9 @@ double oracle_energy_molecule(const oracle_system* s, const oracle_params* p, co
 /* Non-crowder pair energy sum used by Replica::sample (Replica.cpp:1723-1743):
  * sum over chain pairs i<j of E(mol_i, mol_j) with the KH+DH model and no
  * crowder rule (Replica.cpp:793-828). */
+/* Sum of |pair term| of molecule m at mpos against all other molecules. */
+double oracle_energy_molecule_abs(const oracle_system* s, const oracle_params* p,
+                                  const float* pos, int m, const float* mpos);
 double oracle_noncrowder_pair_energy(const oracle_system* s, const oracle_params* p,
                                      const float* pos);
 
