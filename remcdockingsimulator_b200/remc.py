@@ -65,6 +65,8 @@ class Args:
     resume: str = ""
     seed: Optional[int] = None
     sensitivity: bool = False
+    # width (kcal/mol) of the kernel that estimates the bound threshold's term
+    sensitivity_bandwidth: float = 0.25
     autotune: bool = False     # pick threads, layout and cluster size by probe sweeps
     checkpoint_every: int = 0  # MC steps between checkpoints (0: off)
     checkpoint_dir: str = "checkpoints"
@@ -147,6 +149,9 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
         elif t == "--sensitivity":
             a.sensitivity = True
             i += 1
+        elif t == "--sensitivity-bandwidth":
+            a.sensitivity_bandwidth = float(val())
+            i += 2
         elif t == "--autotune":
             a.autotune = True
             i += 1
@@ -165,7 +170,8 @@ def parse_cli(argv: List[str], a: Optional[Args] = None) -> Args:
 
 USAGE = ("Usage: python -m remcdockingsimulator_b200 -f <filename> [-c] [-h] [-v] [-q] [-t x] "
          "[-s x] [-g x] [-m x] [-e x] [-r x] [-o x] [-b x] [-t0 x] [-t1 x] [-bx x] "
-         "[-z checkpoint] [--seed x] [--sensitivity] [--autotune] [--checkpoint-every steps] "
+         "[-z checkpoint] [--seed x] [--sensitivity] [--sensitivity-bandwidth h] [--autotune] "
+         "[--checkpoint-every steps] "
          "[--checkpoint-dir d] [--output-dir d] [--data-dir d]")
 
 _PLACE = re.compile(r"^([tp])\(\s*([^,()]+),\s*([^,()]+),\s*([^,()]+)\)\s*"
@@ -457,7 +463,7 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
         pend_rej = np.zeros(R, np.int64)
         last = [np.zeros(R, np.int64) for _ in range(5)]
         total_ex = total_tests = 0
-        sens = np.zeros((R, 4))  # per temperature: n, sum B, sum X, sum B X (X = dE/dlambda)
+        sens = SensitivitySums(R, a.sensitivity_bandwidth)  # per temperature
         has_crowders = system.n_chains < system.n_mol
         first_block = 1
         if ck is not None:
@@ -465,7 +471,7 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
                               ("tot_acc", tot_acc), ("tot_all", tot_all),
                               ("pend_bound", pend_bound), ("pend_samples", pend_samples),
                               ("pend_acc", pend_acc), ("pend_accA", pend_accA),
-                              ("pend_rej", pend_rej), ("sens", sens)):
+                              ("pend_rej", pend_rej), ("sens", sens.sums)):
                 arr[...] = ck[name]
             total_ex, total_tests = int(ck["total_ex"]), int(ck["total_tests"])
             first_block = int(ck["blocks"]) + 1
@@ -476,7 +482,20 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
         t0 = time.perf_counter()
         step0 = per * (first_block - 1)
         for steps in range(first_block, a.resteps + 1):
-            eng.sweep(per, seed, step0)
+            if a.sensitivity:
+                # one launch per sampling chunk (the same trajectory and the
+                # same samples as one launch per block): B and X = dE/dlambda
+                # at the end of every chunk past sampleafter, as
+                # Replica::sample sees it (main.cpp:975-989)
+                for c in range(per // f):
+                    eng.sweep(f, seed, step0 + c * f)
+                    if step0 + c * f >= a.sample_after:
+                        en = eng.energies()
+                        enc = en + eng.noncrowder_energies() if has_crowders else en
+                        sens.add(eng.temperature_map(), enc, eng.dE_dlambda(),
+                                 2.0 if has_crowders else 1.0)
+            else:
+                eng.sweep(per, seed, step0)
             step0 += per
             n_s, n_b = eng.sample_counters()
             acc, accA, rej = eng.counters()
@@ -499,15 +518,6 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
                         p[6]))
             if dropped:
                 log("-!- %d bound conformations did not fit the record buffer" % dropped)
-            if a.sensitivity:
-                # fluctuation estimate of d<bound>/dlambda from block-end states
-                en = eng.energies()
-                enc = en + eng.noncrowder_energies() if has_crowders else en
-                X = eng.dE_dlambda()
-                tmap = eng.temperature_map()
-                for slot in range(R):
-                    B = 1.0 if enc[slot] < float(BOUND_ENERGY) else 0.0
-                    sens[tmap[slot]] += (1.0, B, X[slot], B * X[slot])
             if steps == a.resteps:
                 break
             tos = eng.temperature_map()
@@ -561,7 +571,7 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
                                  "tot_acc": tot_acc, "tot_all": tot_all,
                                  "pend_bound": pend_bound, "pend_samples": pend_samples,
                                  "pend_acc": pend_acc, "pend_accA": pend_accA,
-                                 "pend_rej": pend_rej, "sens": sens}
+                                 "pend_rej": pend_rej, "sens": sens.sums}
                     save_simulation(a, path, steps, seed, eng.download_state(), eng.energies(),
                                     eng.noncrowder_energies(), eng.temperature_map(), acc_state,
                                     total_ex, total_tests)
@@ -588,12 +598,14 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
         files.close()
         sensitivity = None
         if a.sensitivity:
-            sensitivity = sensitivity_estimates(ladder, sens)
+            sensitivity = sensitivity_estimates(ladder, sens.sums)
             with open(files.base + "_sensitivity", "w") as fh:
-                fh.write("# temperature samples <B> <dE/dlambda> d<B>/dlambda "
-                         "(= -beta (<B X> - <B><X>), X = dE/dlambda, kcal/mol)\n")
-                for T, n, b, x, d in sensitivity:
-                    fh.write("%0.1f %d %.6f %.6f %.6e\n" % (T, n, b, x, d))
+                fh.write("# temperature samples <B> <X> -beta(<BX>-<B><X>) <dB/dlambda> "
+                         "d<B>/dlambda  (B: bound, E_nc < %.4f kcal/mol; X = dE/dlambda, "
+                         "kcal/mol; <dB/dlambda>: threshold term, Gaussian kernel of %.3g "
+                         "kcal/mol)\n" % (float(BOUND_ENERGY), a.sensitivity_bandwidth))
+                for T, n, b, x, cov, surf, d in sensitivity:
+                    fh.write("%0.1f %d %.6f %.6f %.6e %.6e %.6e\n" % (T, n, b, x, cov, surf, d))
         energies = eng.energies()
         log("Simulation: %10.5f ms  (%d exchanges)" % (elapsed * 1000.0, a.resteps))
         return {"elapsed_s": elapsed, "replica_steps": R * per * a.resteps, "e0": e0,
@@ -604,19 +616,64 @@ def simulate(a: Args, system: System, params=None, log=print, on_checkpoint=None
         eng.close()
 
 
+class SensitivitySums:
+    """Per-temperature sums for the fluctuation estimate of d<B>/dlambda.
+
+    B = 1{E_nc < -1.1844 kcal/mol} is the bound indicator of Replica::sample
+    (Replica.cpp:1717-1780, definitions.h:84): E_nc is the potential, plus the
+    chain-chain pair energy when the system has crowders. X = dE/dlambda comes
+    from the adjoint. The energy is linear in lambda (eps = lambda (M - e0)
+    enters each residue pair linearly and crowder terms do not depend on it),
+    and the chain-chain energy is the residue-pair part of E, so
+    dE_nc/dlambda = c X with c = 2 when crowders are present, else 1. In the
+    canonical ensemble at each temperature
+
+        d<B>/dlambda = <dB/dlambda> - beta (<B X> - <B><X>),
+
+    and since B depends on lambda through E_nc, dB/dlambda = -delta(E_nc - thr)
+    c X: a threshold term, estimated with a Gaussian kernel of width h,
+    -(1/n) sum_i K_h(E_nc,i - thr) c X_i. Columns per temperature: n, sum B,
+    sum X, sum B X, sum K_h(E_nc - thr) c X."""
+
+    def __init__(self, n_temps: int, bandwidth: float = 0.25,
+                 threshold: float = float(BOUND_ENERGY)):
+        if not bandwidth > 0.0:
+            raise ArgError("sensitivity bandwidth must be positive")
+        self.sums = np.zeros((n_temps, 5))
+        self.h = float(bandwidth)
+        self.thr = float(threshold)
+
+    def add(self, temp_of_slot, e_nc, X, c: float = 1.0) -> None:
+        """One sample per slot: the temperature index it holds, its E_nc and
+        its dE/dlambda."""
+        t = np.asarray(temp_of_slot, np.int64)
+        e = np.asarray(e_nc, np.float64)
+        x = np.asarray(X, np.float64)
+        B = (e < self.thr).astype(np.float64)
+        u = (e - self.thr) / self.h
+        K = np.exp(-0.5 * u * u) / (self.h * np.sqrt(2.0 * np.pi))
+        cols = np.stack([np.ones_like(x), B, x, B * x, K * c * x], axis=1)
+        np.add.at(self.sums, t, cols)
+
+
 def sensitivity_estimates(ladder: np.ndarray, sums: np.ndarray):
-    """Fluctuation formula d<B>/dtheta = -beta (<B X> - <B><X>), X = dE/dtheta,
-    beta = 4184 / (R T) per kcal/mol, from per-temperature sums
-    (n, sum B, sum X, sum B X). Returns (T, n, <B>, <X>, d<B>/dtheta) rows."""
+    """d<B>/dlambda per temperature from SensitivitySums columns (n, sum B,
+    sum X, sum B X, sum K c X), beta = 4184 / (R T) per kcal/mol. Returns
+    (T, n, <B>, <X>, -beta (<BX> - <B><X>), <dB/dlambda>, d<B>/dlambda) rows;
+    sums with four columns (no threshold term) give a zero threshold term."""
     out = []
+    nan = float("nan")
     for t, T in enumerate(ladder):
-        n, sb, sx, sbx = sums[t]
+        n, sb, sx, sbx = sums[t][:4]
+        skx = sums[t][4] if len(sums[t]) > 4 else 0.0
         if n == 0:
-            out.append((float(T), 0, float("nan"), float("nan"), float("nan")))
+            out.append((float(T), 0, nan, nan, nan, nan, nan))
             continue
         beta = 4184.0 / (float(np.float32(8.314472)) * float(T))
         mb, mx, mbx = sb / n, sx / n, sbx / n
-        out.append((float(T), int(n), mb, mx, -beta * (mbx - mb * mx)))
+        cov = -beta * (mbx - mb * mx)
+        surf = -skx / n
+        out.append((float(T), int(n), mb, mx, cov, surf, cov + surf))
     return out
 
 

@@ -92,7 +92,29 @@ def test_sensitivity_estimator(built_lib):
     X = rng.normal(0.0, 2.0, size=200000)
     B = (X < 0).astype(float)
     sums = np.array([[len(X), B.sum(), X.sum(), (B * X).sum()]])
-    (T, n, mb, mx, d), = remc.sensitivity_estimates(np.array([300.0]), sums)
+    (T, n, mb, mx, cov, surf, d), = remc.sensitivity_estimates(np.array([300.0]), sums)
     beta = 4184.0 / (8.314472 * 300.0)
     assert abs(mb - 0.5) < 0.01
     assert abs(d - beta * 2.0 / np.sqrt(2 * np.pi)) < 0.02 * beta
+    assert surf == 0.0 and d == cov
+
+
+def test_sensitivity_threshold_term(built_lib):
+    """The threshold term <dB/dlambda> = -p(thr) <c X | E_nc = thr>, by the
+    Gaussian kernel: energies N(mu, s^2), so the kernel estimate converges to
+    the density of N(mu, s^2 + h^2) at the threshold; X = dE/dlambda a
+    constant; c = 2 (crowders present)."""
+    from remcdockingsimulator_b200 import remc
+    rng = np.random.default_rng(1)
+    mu, sd, h, x0 = -1.5, 0.8, 0.25, -7.0
+    E = rng.normal(mu, sd, size=400000)
+    acc = remc.SensitivitySums(1, bandwidth=h)
+    acc.add(np.zeros(E.size, np.int64), E, np.full(E.size, x0), c=2.0)
+    (T, n, mb, mx, cov, surf, d), = remc.sensitivity_estimates(np.array([300.0]), acc.sums)
+    thr = float(remc.BOUND_ENERGY)
+    s2 = sd * sd + h * h
+    dens = np.exp(-0.5 * (thr - mu) ** 2 / s2) / np.sqrt(2 * np.pi * s2)
+    assert n == E.size and abs(mb - np.mean(E < thr)) < 1e-12
+    assert abs(cov) < 1e-9  # X does not fluctuate
+    assert abs(surf - (-dens * 2.0 * x0)) < 0.01 * abs(dens * 2.0 * x0)
+    assert abs(d - (cov + surf)) < 1e-12

@@ -101,8 +101,13 @@ def test_driver_writes_reference_output_files(tmp_path, built_lib):
     assert idx[0] == "index molecule_file_path crowder(Y/N)" and idx[-1].endswith(" Y")
     assert summary["replica_steps"] == 6 * 400
     # fluctuation sensitivities: one row per temperature, one sample per
-    # replica per block
+    # replica per sampling chunk (2 chunks of 50 steps per 100-step block);
+    # the total is the covariance term plus the threshold term
     sens = open(base + "_sensitivity").read().splitlines()[1:]
     assert len(sens) == 6
-    assert sum(int(l.split()[1]) for l in sens) == 6 * 4
-    assert all(np.isfinite(float(l.split()[4])) for l in sens if int(l.split()[1]) > 0)
+    assert sum(int(l.split()[1]) for l in sens) == 6 * 4 * 2
+    for l in sens:
+        v = [float(x) for x in l.split()]
+        if int(v[1]) > 0:
+            assert all(np.isfinite(v[4:]))
+            assert abs(v[6] - (v[4] + v[5])) <= 1e-5 * max(abs(v[6]), 1e-6)
