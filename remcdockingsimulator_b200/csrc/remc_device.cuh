@@ -162,6 +162,27 @@ __device__ __forceinline__ float pair_r2(float4 a, float4 b, float L, float invL
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
+// The minimum image folded, scalar (fold_image2 below, one element): the
+// image distance min(|d|, L - |d|) in magnitude, for |d| < 1.5 L.
+__device__ __forceinline__ float fold_image(float d, float L) {
+  const float a = fabsf(d);
+  return fminf(a, __fsub_rn(L, a));
+}
+__device__ __forceinline__ float pair_r2_fold(float4 a, float4 b, float L) {
+  float dx = fold_image(a.x - b.x, L);
+  float dy = fold_image(a.y - b.y, L);
+  float dz = fold_image(a.z - b.z, L);
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+// pair_r2, folded where the caller knows every |d| < 1.5 L (FOLD)
+template <bool FOLD>
+__device__ __forceinline__ float pair_r2_f(float4 a, float4 b, float L, float invL) {
+  if constexpr (FOLD)
+    return pair_r2_fold(a, b, L);
+  else
+    return pair_r2(a, b, L, invL);
+}
+
 // ---------------------------------------------------------------- packed pairs
 // Two pairs per lane in packed FP32 (f32x2: one instruction for both pairs,
 // each element rounded as the scalar operation is). The displacement is taken

@@ -228,7 +228,7 @@ constexpr int kRing = 64;  // proposal records held in shared memory (two halves
 // Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
 // mmax molecules, lmax beads per molecule).
 struct SweepSmem {
-  size_t tab, beads, centres, trial_pos, trial_rel, ring, red, total;
+  size_t tab, beads, centres, trial_pos, ring, red, total;
   static __host__ __device__ size_t take(size_t& off, size_t bytes) {
     size_t o = off;
     off += (bytes + 15) & ~size_t(15);
@@ -245,7 +245,6 @@ struct SweepSmem {
     s.beads = take(off, beads_in_smem ? sizeof(float4) * nmax : 0);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
-    s.trial_rel = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
@@ -294,14 +293,6 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   float4* const sm_beads = reinterpret_cast<float4*>(smem_raw + L.beads);
   float4* s_cent = reinterpret_cast<float4*>(smem_raw + L.centres);
   float4* const sm_tpos = reinterpret_cast<float4*>(smem_raw + L.trial_pos);
-  // rotated relative positions of the chain's beads, computed with its trial
-  // positions by the beads' owners and installed by the same threads: the
-  // install writes rel without reading it, so the CTAs of a cluster, which
-  // all install the same values, cannot read one another's update. Two
-  // buffers by step parity, like the trial positions: the next step's owners
-  // (another molecule, other threads) write theirs before any barrier, while
-  // slower warps may still install from this step's
-  float4* const sm_trel = reinterpret_cast<float4*>(smem_raw + L.trial_rel);
   StepRec* s_ring = reinterpret_cast<StepRec*>(smem_raw + L.ring);
   double* s_red = reinterpret_cast<double*>(smem_raw + L.red);
 
@@ -342,9 +333,21 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   const StepRec* recs = A.recs + (size_t)inst * A.rec_stride + A.rec_offset;
   const int n_steps = A.n_steps;
   float4* const s_beads = GB ? A.pos + bead_off : sm_beads;
-  float4* const s_tpos =
-      GB ? A.trial_scratch + ((size_t)inst * csize + crank) * 4 * (size_t)A.lmax : sm_tpos;
-  float4* const s_trel = GB ? s_tpos + 2 * (size_t)A.lmax : sm_trel;
+  // per-(instance, CTA rank) global scratch of 4 lmax entries: trial
+  // positions (used when the beads stay in global memory) and trial
+  // relative positions
+  float4* const scratch =
+      A.trial_scratch + ((size_t)inst * csize + crank) * 4 * (size_t)A.lmax;
+  float4* const s_tpos = GB ? scratch : sm_tpos;
+  // rotated relative positions of the chain's beads, computed with its trial
+  // positions by the beads' owners and installed by the same threads, so
+  // they need no shared memory: each thread reads back only what it wrote.
+  // The install writes rel without reading it, so the CTAs of a cluster,
+  // which all install the same values, cannot read one another's update.
+  // Two buffers by step parity, like the trial positions: the next step's
+  // owners (another molecule, other threads) write theirs before any
+  // barrier, while slower warps may still install from this step's
+  float4* const s_trel = scratch + 2 * (size_t)A.lmax;
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
@@ -994,8 +997,9 @@ constexpr int kTile = 128;
 // in ascending j: two beads per pass in packed FP32 from the tile's
 // coordinate arrays (an odd first bead, and a last one, alone). FIXED: one
 // table entry for every j (crowders of the system's one species), else the
-// entry of each j's type.
-template <bool R12, bool CUT, bool FIXED>
+// entry of each j's type. FOLD: the folded minimum image (the system's every
+// bead pair is within 1.5 box lengths on each axis).
+template <bool R12, bool CUT, bool FIXED, bool FOLD>
 __device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const float* __restrict__ sy,
                                           const float* __restrict__ sz, const int* __restrict__ st,
                                           const float4* __restrict__ s_tab, int ta, float4 Tfix,
@@ -1006,7 +1010,7 @@ __device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const fl
   if (j < b && ((j - j0) & 1)) {
     const int o = j - j0;
     const float4 T = FIXED ? Tfix : s_tab[st[o] * kNT + ta];
-    acc += crowd_energy<R12, CUT>(pair_r2(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
+    acc += crowd_energy<R12, CUT>(pair_r2_f<FOLD>(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
                                   T.x, T.z);
     ++j;
   }
@@ -1014,7 +1018,7 @@ __device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const fl
 #pragma unroll 2
   for (; j + 1 < b; j += 2) {
     const int o = j - j0;  // even: 8-byte aligned pairs
-    const float2 r2 = pair_r2_2(*reinterpret_cast<const float2*>(sx + o),
+    const float2 r2 = pair_r2_2<FOLD>(*reinterpret_cast<const float2*>(sx + o),
                                 *reinterpret_cast<const float2*>(sy + o),
                                 *reinterpret_cast<const float2*>(sz + o), npx, npy, npz, B);
     float2 A2 = Af, C2 = Cf;
@@ -1030,7 +1034,7 @@ __device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const fl
   if (j < b) {
     const int o = j - j0;
     const float4 T = FIXED ? Tfix : s_tab[st[o] * kNT + ta];
-    acc += crowd_energy<R12, CUT>(pair_r2(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
+    acc += crowd_energy<R12, CUT>(pair_r2_f<FOLD>(pi, make_float4(sx[o], sy[o], sz[o], 0.0f), box, invbox),
                                   T.x, T.z);
   }
 }
@@ -1047,8 +1051,9 @@ __device__ __forceinline__ void crowd_run(const float* __restrict__ sx, const fl
 //                          the system has one crowder species;
 //   crowder i, chain j ... crowder wall, table entry per residue type.
 // The crowder-wall loops take two beads per pass in packed FP32. The single
-// accumulator runs in ascending j, as one unspecialised loop would.
-template <bool R12, bool CUT>
+// accumulator runs in ascending j, as one unspecialised loop would. FOLD: the
+// folded minimum image (the system's fold flag is set).
+template <bool R12, bool CUT, bool FOLD>
 __device__ __forceinline__ void energy_row(const float4* __restrict__ s_j,
                                            const float* __restrict__ sx,
                                            const float* __restrict__ sy,
@@ -1075,20 +1080,20 @@ __device__ __forceinline__ void energy_row(const float4* __restrict__ s_j,
       for (int j = a; j < cb; ++j) {
         const float4 pj = s_j[j - j0];
         const float4 T = s_tab[bead_type(pj.w) * kNT + ta];
-        const float e = pair_energy_r2(pair_r2(pi, pj, box, invbox), T, false, K);
+        const float e = pair_energy_r2(pair_r2_f<FOLD>(pi, pj, box, invbox), T, false, K);
         acc += e;
         acc_cc += e;
       }
     } else {
-      crowd_run<R12, CUT, false>(sx, sy, sz, st, s_tab, ta, Tc, j0, a, cb, pi, npx, npy, npz, B,
+      crowd_run<R12, CUT, false, FOLD>(sx, sy, sz, st, s_tab, ta, Tc, j0, a, cb, pi, npx, npy, npz, B,
                                  box, invbox, acc);
     }
     const int ca = max(a, ncb);
     if (ctype >= 0)
-      crowd_run<R12, CUT, true>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
+      crowd_run<R12, CUT, true, FOLD>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
                                 box, invbox, acc);
     else
-      crowd_run<R12, CUT, false>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
+      crowd_run<R12, CUT, false, FOLD>(sx, sy, sz, st, s_tab, ta, Tc, j0, ca, b, pi, npx, npy, npz, B,
                                  box, invbox, acc);
   }
 }
@@ -1173,8 +1178,11 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     if (__syncthreads_or(!ok)) {  // the copy never landed: report and stop
       if (tid == 0) {
         atomicOr(err, 1);
-        // the next tile's copy writes this CTA's shared memory: let it land
-        // (bounded) before the CTA leaves
+        // both copies this CTA may have in flight write its shared memory:
+        // this item's (the phase just given up on) and the next item's. Wait
+        // for each again, bounded, before the CTA leaves; it can leave with a
+        // copy still in flight only if these waits run out as well
+        mbar_wait(&s_bar[buf], ((phases >> buf) & 1u) ^ 1u, kWaitLimit);
         if (next < n_items) mbar_wait(&s_bar[buf ^ 1], (phases >> (buf ^ 1)) & 1u, kWaitLimit);
       }
       return;
@@ -1193,25 +1201,24 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
       const int ta = bead_type(pi.w);
       const int lo = (W.ti == W.tj) ? i + 1 : j0;
       float acc = 0.0f, acc_cc = 0.0f;  // all pairs; chain-chain pairs
+#define REMC_ENERGY_ROW(R12_, CUT_, FOLD_)                                                      \
+  energy_row<R12_, CUT_, FOLD_>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,          \
+                                S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K, \
+                                acc, acc_cc)
       if (K.crowder_mode) {
-        if (K.crowder_cut)
-          energy_row<true, true>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
-                                 S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
-                                 acc, acc_cc);
-        else
-          energy_row<true, false>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
-                                  S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
-                                  acc, acc_cc);
+        if (K.crowder_cut) {
+          if (S.fold_mi) REMC_ENERGY_ROW(true, true, true); else REMC_ENERGY_ROW(true, true, false);
+        } else {
+          if (S.fold_mi) REMC_ENERGY_ROW(true, false, true); else REMC_ENERGY_ROW(true, false, false);
+        }
       } else {
-        if (K.crowder_cut)
-          energy_row<false, true>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
-                                  S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K,
-                                  acc, acc_cc);
-        else
-          energy_row<false, false>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,
-                                   S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox,
-                                   K, acc, acc_cc);
+        if (K.crowder_cut) {
+          if (S.fold_mi) REMC_ENERGY_ROW(false, true, true); else REMC_ENERGY_ROW(false, true, false);
+        } else {
+          if (S.fold_mi) REMC_ENERGY_ROW(false, false, true); else REMC_ENERGY_ROW(false, false, false);
+        }
       }
+#undef REMC_ENERGY_ROW
       dsum = (double)acc;
       dcc = (double)acc_cc;
     }
@@ -1787,7 +1794,7 @@ struct remc_handle {
   int sweep_csize = 1; // CTAs per replica (thread-block cluster size)
   int sweep_cluster_slots = 0;  // clusters of that size the GPU holds at once
   int beads_in_smem = 1; // beads resident in shared memory (else updated in place in global)
-  float4* d_trial_scratch = nullptr;  // trial buffers when the beads stay in global memory
+  float4* d_trial_scratch = nullptr;  // sweep trial buffers, 4 lmax per (instance, CTA rank)
   float* d_fold_part = nullptr;       // per instance: the fold test's partial extents [8]
   size_t trial_scratch_cap = 0;       // float4 entries
   int max_dyn_smem = 0;
@@ -2009,8 +2016,10 @@ int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize, int
                        cudaGetErrorString(e));
     h->sweep_cluster_slots = clusters;
   }
-  if (!beads_in_smem) {
-    // trial buffers of every (instance, CTA rank): 4 lmax float4 each
+  {
+    // trial buffers of every (instance, CTA rank): 4 lmax float4 each (the
+    // trial relative positions, and the trial positions when the beads stay
+    // in global memory)
     const size_t need = (size_t)h->n_inst * csize * 4 * (size_t)h->lmax;
     if (need > h->trial_scratch_cap) {
       float4* p = nullptr;
