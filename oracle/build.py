@@ -9,6 +9,8 @@ Produces:
                                      + its main.cpp
   oracle/_ref/REMCDockingGPU       - the reference's own GPU build (-DEnableCUDA),
   oracle/_ref/REMCDockingGPU_streams  and its stream build (-DEnableStreams),
+  oracle/_ref/ref_gpu_check          the -c check of the GPU build's main.cpp
+                                     around its own Replica code (ref_gpu_check.cpp),
                                      from the same unmodified sources, with
                                      include/remc_cudaexterns.h force-included
                                      in place of its cudaExterns.h and linked
@@ -141,14 +143,24 @@ def build_reference_gpu(force: bool = False) -> bool:
             if force or _stale(o, [s] + deps):
                 _run(["g++"] + REF_CFLAGS + defs + inc + ["-c", s, "-o", o])
             objs.append(o)
+        # the library is found next to the repository at run time
+        link = ["-pthread", "-L" + libdir, "-lremc_b200", "-L/usr/local/cuda/lib64", "-lcudart",
+                "-L/usr/local/cuda/lib64/stubs", "-lcuda",
+                "-Wl,-rpath,$ORIGIN/../../remcdockingsimulator_b200/lib",
+                "-Wl,-rpath,/usr/local/cuda/lib64"]
         exe = os.path.join(REF_OUT, name)
         if force or _stale(exe, objs + [lib]):
-            # the library is found next to the repository at run time
-            _run(["g++", "-o", exe] + objs +
-                 ["-pthread", "-L" + libdir, "-lremc_b200", "-L/usr/local/cuda/lib64", "-lcudart",
-                  "-L/usr/local/cuda/lib64/stubs", "-lcuda",
-                  "-Wl,-rpath,$ORIGIN/../../remcdockingsimulator_b200/lib",
-                  "-Wl,-rpath,/usr/local/cuda/lib64"])
+            _run(["g++", "-o", exe] + objs + link)
+        if name == "REMCDockingGPU":
+            # the -c check around the reference's own Replica code
+            chk_src = os.path.join(HERE, "ref_gpu_check.cpp")
+            chk_obj = os.path.join(objdir, "ref_gpu_check.o")
+            if force or _stale(chk_obj, [chk_src] + deps):
+                _run(["g++"] + REF_CFLAGS + defs + inc + ["-c", chk_src, "-o", chk_obj])
+            chk = os.path.join(REF_OUT, "ref_gpu_check")
+            unit_objs = [o for o in objs if not o.endswith("main.o")]
+            if force or _stale(chk, unit_objs + [chk_obj, lib]):
+                _run(["g++", "-o", chk] + unit_objs + [chk_obj] + link)
     return True
 
 

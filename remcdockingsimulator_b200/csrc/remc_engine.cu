@@ -1391,13 +1391,16 @@ __device__ __forceinline__ void adjoint_group(
 // exactly the two the first transpose-reduce level combines, so the j forces
 // land in the same registers as in adjoint_group. Coordinates come from the
 // tile's structure-of-arrays copy, so both beads' x (y, z) load straight into
-// one register pair. Works with e = p_j - p_i = -d: the forces it sums are
-// the negated pair forces (the caller negates the i-force sums; the j beads
+// one register pair: gx, gy, gz hold the group's coordinates with beads q
+// and q + 4 side by side (q < 4), in the order this lane's half-warp pairs
+// them (see adjoint_tile_kernel), so each pair is one 8-byte load per
+// coordinate. Works with e = p_j - p_i = -d: the forces it sums are the
+// negated pair forces (the caller negates the i-force sums; the j beads
 // receive them as they are).
 template <bool R12, bool CUT>
 __device__ __forceinline__ void adjoint_group_crowd2(
-    const float* __restrict__ s_jx, const float* __restrict__ s_jy,
-    const float* __restrict__ s_jz, float (*__restrict__ s_fjw)[3], int jg, int jend,
+    const float* __restrict__ gx8, const float* __restrict__ gy8,
+    const float* __restrict__ gz8, float (*__restrict__ s_fjw)[3], int jg, int jend,
     float2 npx, float2 npy, float2 npz, float A, float cut2, float box, float invbox, int lane,
     float2& nfx, float2& nfy, float2& nfz, float2& acc_e2) {
   const int r = (lane >> 2) & 7;
@@ -1409,10 +1412,11 @@ __device__ __forceinline__ void adjoint_group_crowd2(
   float g[8][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int ja = jg + (q ^ r), jb = jg + ((q + 4) ^ r);
-    float2 ex = __fadd2_rn(make_float2(s_jx[ja], s_jx[jb]), npx);
-    float2 ey = __fadd2_rn(make_float2(s_jy[ja], s_jy[jb]), npy);
-    float2 ez = __fadd2_rn(make_float2(s_jz[ja], s_jz[jb]), npz);
+    // beads jg + (q ^ r) and jg + ((q + 4) ^ r), in that order
+    const int o = 2 * ((q ^ r) & 3);
+    float2 ex = __fadd2_rn(*reinterpret_cast<const float2*>(gx8 + o), npx);
+    float2 ey = __fadd2_rn(*reinterpret_cast<const float2*>(gy8 + o), npy);
+    float2 ez = __fadd2_rn(*reinterpret_cast<const float2*>(gz8 + o), npz);
     ex = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ex, iL, M), nM), ex);
     ey = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ey, iL, M), nM), ey);
     ez = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ez, iL, M), nM), ez);
@@ -1473,7 +1477,13 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
     double* __restrict__ e_out, EnergyConsts K, AdjConsts C) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
-  __shared__ float s_jx[kTile], s_jy[kTile], s_jz[kTile];  // the j tile again, by coordinate
+  // the tile's crowder part [jc, jn) again, by coordinate, in groups of 8
+  // from jc with beads q and q + 4 side by side: copy 0 in the order
+  // (q, q + 4) for lanes 0-15, copy 1 in the order (q + 4, q) for lanes 16-31
+  // (adjoint_group's bead order j = jg + (q ^ r), r = (lane >> 2) & 7, puts
+  // the bead of the pair with the smaller index first for r < 4, last for
+  // r >= 4). 8 entries of slack: a partial last group is stored, not read
+  __shared__ __align__(16) float s_px[2][kTile + 8], s_py[2][kTile + 8], s_pz[2][kTile + 8];
   __shared__ float s_fj[kTile / 32][kTile][3];
   __shared__ float s_G[kNumAmino * kNumAmino];
   __shared__ double s_red[kTile / 32][2];
@@ -1487,13 +1497,21 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
     const float box = S.box, invbox = S.invbox;
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
+    const int jc = max(0, min(jn, S.n_chain_beads - j0));  // [0, jc) residues, [jc, jn) crowders
     __syncthreads();  // the previous item is done with the shared buffers
     if (tid < jn) {
       const float4 p = pos[base + j0 + tid];
       s_j[tid] = p;
-      s_jx[tid] = p.x;
-      s_jy[tid] = p.y;
-      s_jz[tid] = p.z;
+      if (tid >= jc) {
+        const int o = tid - jc, w = o & 7, g = (o & ~7) + 2 * (w & 3);
+        const int p0 = g + (w >> 2), p1 = g + 1 - (w >> 2);
+        s_px[0][p0] = p.x;
+        s_py[0][p0] = p.y;
+        s_pz[0][p0] = p.z;
+        s_px[1][p1] = p.x;
+        s_py[1][p1] = p.y;
+        s_pz[1][p1] = p.z;
+      }
     }
     for (int k = tid; k < (kTile / 32) * kTile * 3; k += kTile) (&s_fj[0][0][0])[k] = 0.0f;
     for (int k = tid; k < kNumAmino * kNumAmino; k += kTile) s_G[k] = 0.0f;
@@ -1511,8 +1529,8 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
       ex0 = mol_start[S.mstart_off + mi] - j0;
       ex1 = mol_start[S.mstart_off + mi + 1] - j0;
     }
-    const int jc = max(0, min(jn, S.n_chain_beads - j0));  // [0, jc) residues, [jc, jn) crowders
     const bool tc_fixed = S.crowd_type >= 0;
+    const int half = lane >> 4;
     const float4 Tc = s_tab[(tc_fixed ? S.crowd_type : 0) * kNT + ta];
     float fx = 0.f, fy = 0.f, fz = 0.f, acc_e = 0.f, acc_x = 0.f;
     // packed crowder groups: negated force sums and energy, two pairs per lane
@@ -1538,8 +1556,10 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
       for (int jg = jc; jg < jn; jg += 8) {
         const bool clean = ivalid && jg + 8 <= jn && jg >= jlo && (ex1 <= jg || ex0 >= jg + 8);
         if (__all_sync(0xffffffffu, clean))
-          adjoint_group_crowd2<R12, CUT>(s_jx, s_jy, s_jz, s_fj[warp], jg, jn, npx, npy, npz,
-                                         Tc.x, Tc.z, box, invbox, lane, nfx, nfy, nfz, acc_e2);
+          adjoint_group_crowd2<R12, CUT>(s_px[half] + (jg - jc), s_py[half] + (jg - jc),
+                                         s_pz[half] + (jg - jc), s_fj[warp], jg, jn, npx, npy,
+                                         npz, Tc.x, Tc.z, box, invbox, lane, nfx, nfy, nfz,
+                                         acc_e2);
         else
           adjoint_group<R12, CUT, false, true>(s_j, s_tab, s_G, s_fj[warp], jg, jn, jlo, ex0, ex1,
                                                ivalid, pi, ta, a_crowd, Tc, tc_fixed, box, invbox,

@@ -6,7 +6,11 @@ library through include/remc_cudaexterns.h, run on the B200:
   * its -c check (simulation engine/src/main.cpp:1652-1707): Replica::E() on
     the CPU against Replica::EonDevice() (Replica.cpp:1601-1616, here
     CUDA_EonDevice of libremc_b200.so) on the ten docked reference structures,
-    printed as "CPU,GPU,err";
+    printed as "CPU,GPU,err". The check runs through oracle/ref_gpu_check.cpp,
+    the same sequence around the reference's own Replica code with the
+    molecule array reserved first: main.cpp's check crashes on the CPU side
+    before any GPU work (its stack Replicas delete an uninitialised array
+    pointer in Replica::loadMolecule, Replica.cpp:229-245);
   * its start-up check (main.cpp:1745-1797), which warns above 1% relative
     error, followed by a short REMC run whose every Monte Carlo step takes its
     energy from this library (Replica::MCSearch, Replica.cpp:422-426; the
@@ -26,7 +30,7 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = {b: os.path.join(ROOT, "oracle", "_ref", b)
-       for b in ("REMCDockingGPU", "REMCDockingGPU_streams")}
+       for b in ("REMCDockingGPU", "REMCDockingGPU_streams", "ref_gpu_check")}
 E_RTOL = 1e-5
 
 
@@ -59,10 +63,10 @@ def _run(build, args, cwd, timeout=600):
 
 
 def test_reference_check_mode_through_this_library(golden, golden_table, tmp_path, built_lib):
-    _need("REMCDockingGPU")
+    _need("ref_gpu_check")
     d = str(tmp_path)
     _write_inputs(d, golden, golden_table)
-    out = _run("REMCDockingGPU", ["-c"], d)
+    out = _run("ref_gpu_check", [], d)
     rows = [tuple(float(x) for x in m.groups())
             for m in re.finditer(r"CPU,GPU,err:\s+(\S+)\s+(\S+)\s+(\S+)", out)]
     assert len(rows) == 10, out[-3000:]
@@ -86,8 +90,10 @@ def test_reference_startup_check_and_run_through_this_library(build, golden, gol
     cfg = os.path.join(d, "config")
     with open(cfg, "w") as fh:
         fh.write("\n".join([
+            # sampleafter > 0: the stream build's loop takes the step modulo
+            # sampleafter (main.cpp:1042)
             "gpus 1", "streams %d" % threads, "threads %d" % threads, "mcsteps 400",
-            "resteps 4", "replicas 4", "samplefrequency 10", "sampleafter 0", "boundry 118.4",
+            "resteps 4", "replicas 4", "samplefrequency 10", "sampleafter 100", "boundry 118.4",
             "temperaturemax 360", "temperaturemin 300", "prefix dropin", "files",
             # structure 3: the chains in contact, E = -10.28 kcal/mol; t(0,0,0)
             # keeps the file's coordinates, angle -1 means no rotation
