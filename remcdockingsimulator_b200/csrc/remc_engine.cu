@@ -218,7 +218,7 @@ struct SweepArgs {
   int mol_in_smem;       // centres resident in shared memory
   int csize;             // CTAs per replica (a thread-block cluster), 1, 2, 4 or 8
   // beads kept in global memory (systems too large for shared memory): trial
-  // positions and trial relative positions of each (instance, CTA rank), 4 lmax
+  // positions and trial relative positions of each (instance, CTA rank), 6 lmax
   float4* trial_scratch;
   EnergyConsts K;
 };
@@ -244,7 +244,7 @@ struct SweepSmem {
     s.tab = take(off, sizeof(float4) * kNT * kNT);
     s.beads = take(off, beads_in_smem ? sizeof(float4) * nmax : 0);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
-    s.trial_pos = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
+    s.trial_pos = take(off, beads_in_smem ? sizeof(float4) * 4 * lmax : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
@@ -333,11 +333,16 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   const StepRec* recs = A.recs + (size_t)inst * A.rec_stride + A.rec_offset;
   const int n_steps = A.n_steps;
   float4* const s_beads = GB ? A.pos + bead_off : sm_beads;
-  // per-(instance, CTA rank) global scratch of 4 lmax entries: trial
+  // per-(instance, CTA rank) global scratch of 6 lmax entries: trial
   // positions (used when the beads stay in global memory) and trial
   // relative positions
   float4* const scratch =
-      A.trial_scratch + ((size_t)inst * csize + crank) * 4 * (size_t)A.lmax;
+      A.trial_scratch + ((size_t)inst * csize + crank) * 6 * (size_t)A.lmax;
+  // trial positions of a chain move, two entries per moved bead k, by step
+  // parity b: s_tpos[2 (b lmax + k)] = (new x, old x, new y, old y),
+  // s_tpos[2 (b lmax + k) + 1] = (new z, old z, meta word, table row offset),
+  // so that each (new, old) coordinate pair is a register pair of the packed
+  // pair loops as loaded
   float4* const s_tpos = GB ? scratch : sm_tpos;
   // rotated relative positions of the chain's beads, computed with its trial
   // positions by the beads' owners and installed by the same threads, so
@@ -347,7 +352,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   // Two buffers by step parity, like the trial positions: the next step's
   // owners (another molecule, other threads) write theirs before any
   // barrier, while slower warps may still install from this step's
-  float4* const s_trel = scratch + 2 * (size_t)A.lmax;
+  float4* const s_trel = scratch + 4 * (size_t)A.lmax;
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
@@ -386,9 +391,27 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     cooperative_groups::this_cluster().sync();
   else
     __syncthreads();
-  // centre of the next step's molecule when centres live in global memory
-  float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (n_steps > 0 && !A.mol_in_smem) next_c = cent[s_ring[0].m];
+  // the next step's record fields, its molecule's centre and, for a
+  // one-bead molecule, its bead, loaded one step ahead (right after the
+  // previous step's barrier) so that a step starts without waiting on them.
+  // A molecule that the current step moves and accepts is taken from
+  // registers in the next step instead (same), so the early loads never
+  // need a value the current step writes.
+  int nx_m = 0, nx_m0 = 0, nx_info = 0;
+  float nx_t0 = 0.f, nx_t1 = 0.f, nx_t2 = 0.f;
+  float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f), next_b = next_c;
+  auto load_next = [&](int step) {
+    const StepRec& r = s_ring[step & (kRing - 1)];
+    nx_m = r.m;
+    nx_m0 = r.m0;
+    nx_info = r.info;
+    nx_t0 = r.t[0];
+    nx_t1 = r.t[1];
+    nx_t2 = r.t[2];
+    next_c = cent[nx_m];
+    if ((nx_info & kRecCount) == 1) next_b = s_beads[nx_m0];
+  };
+  if (n_steps > 0) load_next(0);
 
   // previous step, known to every thread
   int p_m = -1, p_acc = 0, p_rot = 0, p_n = 0, p_b = 0;
@@ -414,14 +437,15 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       int m, rotate, crowd;
       float t[3];
     } rec;
-    rec.m = recs_.m;
-    rec.rotate = (recs_.info & kRecRotate) != 0;
-    rec.crowd = (recs_.info & kRecCrowd) != 0;
-    rec.t[0] = recs_.t[0];
-    rec.t[1] = recs_.t[1];
-    rec.t[2] = recs_.t[2];
+    rec.m = nx_m;
+    rec.rotate = (nx_info & kRecRotate) != 0;
+    rec.crowd = (nx_info & kRecCrowd) != 0;
+    rec.t[0] = nx_t0;
+    rec.t[1] = nx_t1;
+    rec.t[2] = nx_t2;
     const int m = rec.m;
-    const int m0 = recs_.m0, n = recs_.info & kRecCount;
+    const int m0 = nx_m0, n = nx_info & kRecCount;
+    const float4 this_b = next_b;
     const int b = s & 1;
     const bool same = (m == p_m) && p_acc;  // moved (and accepted) last step
     // centre of m: the one this step's thread computed last step if m moved
@@ -432,7 +456,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       c1 = p_nc1;
       c2 = p_nc2;
     } else {
-      const float4 c = A.mol_in_smem ? cent[m] : next_c;
+      const float4 c = next_c;
       c0 = c.x;
       c1 = c.y;
       c2 = c.z;
@@ -459,7 +483,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     const bool skip = rec.rotate && n == 1;
     float4 pold1, pnew1;  // one-bead molecule: old/new position in registers
     if (n == 1) {
-      pold1 = same ? p_single : s_beads[m0];
+      pold1 = same ? p_single : this_b;
       pnew1 = make_float4(nc0, nc1, nc2, pold1.w);
     } else {
       // trial positions of the chain, built by the owners of its beads
@@ -469,16 +493,20 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       for (; j < m0 + n; j += nthr) {
         const int k = j - m0;
         const float4 rl = A.rel[bead_off + j];
-        const float w = s_beads[j].w;
+        // the bead's current position: this thread owns it and installed
+        // its last move itself
+        const float4 ol = s_beads[j];
         float4 np;
         if (rec.rotate) {
           const float3 r2 = rotate_rel(qp, rl.x, rl.y, rl.z);
-          np = make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), w);
+          np = make_float4(__fadd_rn(r2.x, nc0), __fadd_rn(r2.y, nc1), __fadd_rn(r2.z, nc2), ol.w);
           s_trel[b * A.lmax + k] = make_float4(r2.x, r2.y, r2.z, 0.0f);
         } else {
-          np = make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), w);
+          np = make_float4(__fadd_rn(rl.x, nc0), __fadd_rn(rl.y, nc1), __fadd_rn(rl.z, nc2), ol.w);
         }
-        s_tpos[b * A.lmax + k] = np;
+        float4* e = s_tpos + 2 * (b * A.lmax + k);
+        e[0] = make_float4(np.x, ol.x, np.y, ol.y);
+        e[1] = make_float4(np.z, ol.z, ol.w, __int_as_float(bead_type(ol.w) * kNT));
       }
       __syncthreads();  // trial positions and the previous chain update visible
     }
@@ -568,8 +596,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         // runs over the n moved beads k, the same k in every lane. Two j per
         // pass where the class has them, so each k's positions and table row
         // serve two beads; each j's sum over k is added on its own, in j order
-        const float4* oldp = same ? s_tpos + p_b * A.lmax : s_beads + m0;
-        const float4* newp = s_tpos + b * A.lmax;
+        const float4* tp = s_tpos + 2 * b * A.lmax;
         for (int part = 0; part < 2; ++part) {
           const int lo = part ? x1 : 0, hi = part ? N : x0;
           if (lo >= hi) continue;
@@ -590,10 +617,10 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
                              nbz = make_float2(-pb.z, -pb.z);
                 float a = 0.0f, c = 0.0f;
                 for (int k = 0; k < n; ++k) {
-                  const float4 po = oldp[k], pn = newp[k];
-                  const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
-                               kz = make_float2(pn.z, po.z);
-                  const float4* row = s_tab + bead_type(po.w) * kNT;
+                  const float4 P = tp[2 * k], Q = tp[2 * k + 1];
+                  const float2 kx = make_float2(P.x, P.y), ky = make_float2(P.z, P.w),
+                               kz = make_float2(Q.x, Q.y);
+                  const float4* row = s_tab + __float_as_int(Q.w);
                   const float4 Ta = row[ta], Tb = row[tb];
                   const float2 ea =
                       kh_energy2(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PB), Ta, A.K.c_xi);
@@ -614,8 +641,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             float a = 0.0f;
             if (!rec.crowd) {
               for (int k = 0; k < n; ++k) {
-                const float4 po = oldp[k], pn = newp[k];
-                const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+                const float4 P = tp[2 * k], Q = tp[2 * k + 1];
+                const float4 pn = make_float4(P.x, P.z, Q.x, 0.0f), po = make_float4(P.y, P.w, Q.y, 0.0f);
+                const float4 T = s_tab[__float_as_int(Q.w) + tb];
                 const float en = pair_energy_r2(pair_r2(pn, pj, box, invbox), T, false, A.K);
                 const float eo = pair_energy_r2(pair_r2(po, pj, box, invbox), T, false, A.K);
                 a += en - eo;
@@ -623,8 +651,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
               acc_c += a;
             } else {
               for (int k = 0; k < n; ++k) {
-                const float4 po = oldp[k], pn = newp[k];
-                const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+                const float4 P = tp[2 * k], Q = tp[2 * k + 1];
+                const float4 pn = make_float4(P.x, P.z, Q.x, 0.0f), po = make_float4(P.y, P.w, Q.y, 0.0f);
+                const float4 T = s_tab[__float_as_int(Q.w) + tb];
                 const float en = crowd_energy<R12, CUT>(pair_r2(pn, pj, box, invbox), T.x, T.z);
                 const float eo = crowd_energy<R12, CUT>(pair_r2(po, pj, box, invbox), T.x, T.z);
                 a += en - eo;
@@ -645,10 +674,10 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
                            nbz = make_float2(-pb.z, -pb.z);
               float a = 0.0f, c = 0.0f;
               for (int k = 0; k < n; ++k) {
-                const float4 po = oldp[k], pn = newp[k];
-                const float2 kx = make_float2(pn.x, po.x), ky = make_float2(pn.y, po.y),
-                             kz = make_float2(pn.z, po.z);
-                const float4* row = s_tab + bead_type(po.w) * kNT;
+                const float4 P = tp[2 * k], Q = tp[2 * k + 1];
+                const float2 kx = make_float2(P.x, P.y), ky = make_float2(P.z, P.w),
+                             kz = make_float2(Q.x, Q.y);
+                const float4* row = s_tab + __float_as_int(Q.w);
                 const float4 Ta = row[ta];
                 const float4 Tb = one_ct ? Ta : row[tb];  // one crowder species: ta == tb
                 const float2 ea = crowd_energy2<R12, CUT>(pair_r2_2<F>(kx, ky, kz, nax, nay, naz, PBc),
@@ -670,8 +699,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             const int tb = bead_type(pj.w);
             float a = 0.0f;
             for (int k = 0; k < n; ++k) {
-              const float4 po = oldp[k], pn = newp[k];
-              const float4 T = s_tab[bead_type(po.w) * kNT + tb];
+              const float4 P = tp[2 * k], Q = tp[2 * k + 1];
+              const float4 pn = make_float4(P.x, P.z, Q.x, 0.0f), po = make_float4(P.y, P.w, Q.y, 0.0f);
+              const float4 T = s_tab[__float_as_int(Q.w) + tb];
               const float en = crowd_energy<R12, CUT>(pair_r2(pn, pj, box, invbox), T.x, T.z);
               const float eo = crowd_energy<R12, CUT>(pair_r2(po, pj, box, invbox), T.x, T.z);
               a += en - eo;
@@ -707,11 +737,11 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
 
     // ---- every thread: the same FP64 sums (a fixed pairwise tree over the
     // warps' partials) and the same Metropolis decision
-    if (s + 1 < n_steps && A.mol_in_smem == 0) {
-      // centre of the next step's molecule, loaded while this step finishes;
-      // if that molecule moves in this step, the next step takes the centre
-      // from registers instead (same && !p_rot)
-      next_c = cent[s_ring[(s + 1) & (kRing - 1)].m];
+    if (s + 1 < n_steps) {
+      // the next step's record, centre and bead, loaded while this step
+      // finishes; if that molecule moves in this step, the next step takes
+      // its centre and bead from registers instead (same)
+      load_next(s + 1);
     }
     double dE = tree_sum8(s_red + b * csize * 64);
     double dE_cc = 0.0;
@@ -732,7 +762,9 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
         // the owners install the chain (and its relative positions)
         int j = m0 + ((tid - m0) & tmask);
         for (; j < m0 + n; j += nthr) {
-          s_beads[j] = s_tpos[b * A.lmax + (j - m0)];
+          const float4* e = s_tpos + 2 * (b * A.lmax + (j - m0));
+          const float4 P = e[0], Q = e[1];
+          s_beads[j] = make_float4(P.x, P.z, Q.x, Q.z);
           if (rec.rotate) A.rel[bead_off + j] = s_trel[b * A.lmax + (j - m0)];
         }
       }
@@ -1115,11 +1147,14 @@ __device__ __forceinline__ const float4* tile_src(const SysDev* __restrict__ sys
   return pos + S.bead_base + (W.inst - S.inst0) * N + j0;
 }
 
-// Two-stage pipeline over the CTA's items: while item k is computed, the
-// bulk copy (TMA, no multicast) of item k+1's j-tile lands in the other
-// buffer, and each thread's i-bead loads are issued before it waits for its
-// own tile. A buffer is refilled only after the barrier that ends the item
-// which read it.
+// Two-stage pipeline over the CTA's items with one CTA barrier per item:
+// while item k is computed, the bulk copy (TMA, no multicast) of item k+1's
+// j-tile lands in the other buffer. Item k's barrier, after every thread's
+// own wait for its tile and its share of the by-coordinate copy, also shows
+// that every thread has finished item k-1: only then does thread 0 issue the
+// copy into item k-1's buffer and add up item k-1's warp partials. The
+// by-coordinate copies and the warp partials are double-buffered like the
+// tiles.
 __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
@@ -1127,11 +1162,12 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K,
     int* __restrict__ err) {
   __shared__ float4 s_tab[kNT * kNT];
-  __shared__ __align__(128) float4 s_j[2][kTile];                         // two stages
-  __shared__ __align__(16) float s_jx[kTile], s_jy[kTile], s_jz[kTile];  // the tile by coordinate
-  __shared__ int s_jt[kTile];                                              // and its bead types
-  __shared__ double s_red[kTile / 32];
-  __shared__ double s_red_cc[kTile / 32];
+  __shared__ __align__(128) float4 s_j[2][kTile];  // two stages
+  // the tile by coordinate, and its bead types, per stage
+  __shared__ __align__(16) float s_jx[2][kTile], s_jy[2][kTile], s_jz[2][kTile];
+  __shared__ int s_jt[2][kTile];
+  __shared__ double s_red[2][kTile / 32];
+  __shared__ double s_red_cc[2][kTile / 32];
   __shared__ __align__(8) unsigned long long s_bar[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
@@ -1147,6 +1183,7 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
   __syncthreads();  // barriers initialised
   unsigned phases = 0;  // bit b: parity of buffer b's next completion
   int buf = 0;
+  int prev = -1;  // the previous item, whose partials thread 0 writes out
   for (int it = blockIdx.x; it < n_items; it += gridDim.x, buf ^= 1) {
     const TileItem W = items[it];
     const SysDev S = sys[inst_sys[W.inst]];
@@ -1165,46 +1202,55 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
       xa = mol_start[S.mstart_off + mi];
       xb = mol_start[S.mstart_off + mi + 1];
     }
-    // the next item's tile into the other buffer (its last reader, the
-    // previous item, ended at that item's final barrier)
-    const int next = it + (int)gridDim.x;
-    if (tid == 0 && next < n_items) {
-      unsigned bytes;
-      const float4* src = tile_src(sys, inst_sys, pos, items[next], &bytes);
-      bulk_load(s_j[buf ^ 1], src, bytes, &s_bar[buf ^ 1]);
-    }
     const bool ok = mbar_wait(&s_bar[buf], (phases >> buf) & 1u, kWaitLimit);
     phases ^= 1u << buf;
+    const float4* tile = s_j[buf];
+    if (ok && tid < jn) {
+      const float4 p = tile[tid];
+      s_jx[buf][tid] = p.x;
+      s_jy[buf][tid] = p.y;
+      s_jz[buf][tid] = p.z;
+      s_jt[buf][tid] = bead_type(p.w);
+    }
+    // this item's coordinate copy is complete and every thread is done with
+    // the previous item (its tile buffer, coordinate copy and partials)
     if (__syncthreads_or(!ok)) {  // the copy never landed: report and stop
       if (tid == 0) {
         atomicOr(err, 1);
-        // both copies this CTA may have in flight write its shared memory:
-        // this item's (the phase just given up on) and the next item's. Wait
-        // for each again, bounded, before the CTA leaves; it can leave with a
-        // copy still in flight only if these waits run out as well
+        // the copy given up on still writes this CTA's shared memory (the
+        // next one is not issued yet): wait for it again, bounded, before
+        // the CTA leaves; it can leave with the copy in flight only if this
+        // wait runs out as well
         mbar_wait(&s_bar[buf], ((phases >> buf) & 1u) ^ 1u, kWaitLimit);
-        if (next < n_items) mbar_wait(&s_bar[buf ^ 1], (phases >> (buf ^ 1)) & 1u, kWaitLimit);
       }
       return;
     }
-    const float4* tile = s_j[buf];
-    if (tid < jn) {
-      const float4 p = tile[tid];
-      s_jx[tid] = p.x;
-      s_jy[tid] = p.y;
-      s_jz[tid] = p.z;
-      s_jt[tid] = bead_type(p.w);
+    const int next = it + (int)gridDim.x;
+    if (tid == 0) {
+      if (prev >= 0) {
+        double v = 0.0, c = 0.0;
+        for (int w = 0; w < kTile / 32; ++w) {
+          v += s_red[buf ^ 1][w];
+          c += s_red_cc[buf ^ 1][w];
+        }
+        scratch[prev] = v;
+        scratch_cc[prev] = c;
+      }
+      if (next < n_items) {
+        unsigned bytes;
+        const float4* src = tile_src(sys, inst_sys, pos, items[next], &bytes);
+        bulk_load(s_j[buf ^ 1], src, bytes, &s_bar[buf ^ 1]);
+      }
     }
-    __syncthreads();
     double dsum = 0.0, dcc = 0.0;
     if (ivalid) {
       const int ta = bead_type(pi.w);
       const int lo = (W.ti == W.tj) ? i + 1 : j0;
       float acc = 0.0f, acc_cc = 0.0f;  // all pairs; chain-chain pairs
-#define REMC_ENERGY_ROW(R12_, CUT_, FOLD_)                                                      \
-  energy_row<R12_, CUT_, FOLD_>(tile, s_jx, s_jy, s_jz, s_jt, j0, lo, j0 + jn, xa, xb,          \
-                                S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box, S.invbox, K, \
-                                acc, acc_cc)
+#define REMC_ENERGY_ROW(R12_, CUT_, FOLD_)                                                        \
+  energy_row<R12_, CUT_, FOLD_>(tile, s_jx[buf], s_jy[buf], s_jz[buf], s_jt[buf], j0, lo, j0 + jn, \
+                                xa, xb, S.n_chain_beads, S.crowd_type, pi, ta, s_tab, S.box,     \
+                                S.invbox, K, acc, acc_cc)
       if (K.crowder_mode) {
         if (K.crowder_cut) {
           if (S.fold_mi) REMC_ENERGY_ROW(true, true, true); else REMC_ENERGY_ROW(true, true, false);
@@ -1225,19 +1271,20 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     dsum = warp_sum(dsum);
     dcc = warp_sum(dcc);
     if (lane == 0) {
-      s_red[warp] = dsum;
-      s_red_cc[warp] = dcc;
+      s_red[buf][warp] = dsum;
+      s_red_cc[buf][warp] = dcc;
     }
-    __syncthreads();  // ends the item: its tile buffer and coordinate arrays are free
-    if (tid == 0) {
-      double v = 0.0, c = 0.0;
-      for (int w = 0; w < kTile / 32; ++w) {
-        v += s_red[w];
-        c += s_red_cc[w];
-      }
-      scratch[it] = v;
-      scratch_cc[it] = c;
+    prev = it;
+  }
+  __syncthreads();  // the last item's partials are written
+  if (tid == 0 && prev >= 0) {
+    double v = 0.0, c = 0.0;
+    for (int w = 0; w < kTile / 32; ++w) {
+      v += s_red[buf ^ 1][w];
+      c += s_red_cc[buf ^ 1][w];
     }
+    scratch[prev] = v;
+    scratch_cc[prev] = c;
   }
 }
 
@@ -1610,56 +1657,37 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
 }
 
 // Per-molecule force and torque about the centre (torque = sum rel x F):
-// one CTA per instance; one thread per one-bead molecule, one warp per chain
-// (FP64 sums).
-__global__ void molecule_force_torque_kernel(const SysDev* __restrict__ sys,
-                                             const int* __restrict__ inst_sys,
-                                             const int* __restrict__ mol_start,
-                                             const float4* __restrict__ rel,
-                                             const float* __restrict__ forces,
-                                             double* __restrict__ out) {
+// one thread per molecule, grid (instance, molecule chunk). A one-bead
+// molecule is a copy widened to FP64; a chain's thread sums its beads in
+// order (FP64). Memory-bound: forces, rel and the six doubles per molecule.
+__global__ void __launch_bounds__(128) molecule_force_torque_kernel(
+    const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
+    const int* __restrict__ mol_start, const float4* __restrict__ rel,
+    const float* __restrict__ forces, double* __restrict__ out) {
   const int inst = blockIdx.x;
   const SysDev S = sys[inst_sys[inst]];
+  const int m = blockIdx.y * blockDim.x + threadIdx.x;
+  if (m >= S.n_mol) return;
   const int slot = inst - S.inst0;
   const int base = S.bead_base + slot * S.n_beads;
-  const int mbase = S.mol_base + slot * S.n_mol;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int* ms = mol_start + S.mstart_off;
-  // one-bead molecules (crowders): one thread each, no reduction
-  for (int m = threadIdx.x; m < S.n_mol; m += blockDim.x) {
-    const int a = ms[m];
-    if (ms[m + 1] - a != 1) continue;
-    const float4 rl = rel[base + a];
-    const double Fx = forces[3 * (size_t)(base + a)], Fy = forces[3 * (size_t)(base + a) + 1],
-                 Fz = forces[3 * (size_t)(base + a) + 2];
-    double* o = out + 6 * (size_t)(mbase + m);
-    o[0] = Fx;
-    o[1] = Fy;
-    o[2] = Fz;
-    o[3] = (double)rl.y * Fz - (double)rl.z * Fy;
-    o[4] = (double)rl.z * Fx - (double)rl.x * Fz;
-    o[5] = (double)rl.x * Fy - (double)rl.y * Fx;
+  const int a = ms[m], b = ms[m + 1];
+  double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+  for (int k = a; k < b; ++k) {
+    const float4 rl = rel[base + k];
+    const double Fx = forces[3 * (size_t)(base + k)], Fy = forces[3 * (size_t)(base + k) + 1],
+                 Fz = forces[3 * (size_t)(base + k) + 2];
+    fx += Fx;
+    fy += Fy;
+    fz += Fz;
+    tx += (double)rl.y * Fz - (double)rl.z * Fy;
+    ty += (double)rl.z * Fx - (double)rl.x * Fz;
+    tz += (double)rl.x * Fy - (double)rl.y * Fx;
   }
-  // chains: one warp each
-  for (int m = warp; m < S.n_mol; m += nw) {
-    const int a = ms[m], b = ms[m + 1];
-    if (b - a == 1) continue;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    for (int k = a + lane; k < b; k += 32) {
-      const float4 rl = rel[base + k];
-      const double Fx = forces[3 * (size_t)(base + k)], Fy = forces[3 * (size_t)(base + k) + 1],
-                   Fz = forces[3 * (size_t)(base + k) + 2];
-      v[0] += Fx;
-      v[1] += Fy;
-      v[2] += Fz;
-      v[3] += (double)rl.y * Fz - (double)rl.z * Fy;
-      v[4] += (double)rl.z * Fx - (double)rl.x * Fz;
-      v[5] += (double)rl.x * Fy - (double)rl.y * Fx;
-    }
-    for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
-    if (lane == 0)
-      for (int c = 0; c < 6; ++c) out[6 * (size_t)(mbase + m) + c] = v[c];
-  }
+  double2* o = reinterpret_cast<double2*>(out + 6 * (size_t)(S.mol_base + slot * S.n_mol + m));
+  o[0] = make_double2(fx, fy);
+  o[1] = make_double2(fz, tx);
+  o[2] = make_double2(ty, tz);
 }
 
 // ------------------------------------------------------------------ exchange
@@ -1814,7 +1842,7 @@ struct remc_handle {
   int sweep_csize = 1; // CTAs per replica (thread-block cluster size)
   int sweep_cluster_slots = 0;  // clusters of that size the GPU holds at once
   int beads_in_smem = 1; // beads resident in shared memory (else updated in place in global)
-  float4* d_trial_scratch = nullptr;  // sweep trial buffers, 4 lmax per (instance, CTA rank)
+  float4* d_trial_scratch = nullptr;  // sweep trial buffers, 6 lmax per (instance, CTA rank)
   float* d_fold_part = nullptr;       // per instance: the fold test's partial extents [8]
   size_t trial_scratch_cap = 0;       // float4 entries
   int max_dyn_smem = 0;
@@ -2037,10 +2065,10 @@ int configure_sweep(remc_handle* h, int threads, int mol_in_smem, int csize, int
     h->sweep_cluster_slots = clusters;
   }
   {
-    // trial buffers of every (instance, CTA rank): 4 lmax float4 each (the
+    // trial buffers of every (instance, CTA rank): 6 lmax float4 each (the
     // trial relative positions, and the trial positions when the beads stay
     // in global memory)
-    const size_t need = (size_t)h->n_inst * csize * 4 * (size_t)h->lmax;
+    const size_t need = (size_t)h->n_inst * csize * 6 * (size_t)h->lmax;
     if (need > h->trial_scratch_cap) {
       float4* p = nullptr;
       if (dev_alloc(&p, need)) return REMC_ERR_NOMEM;
@@ -2911,17 +2939,22 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
   C.inv_xi = 1.0f / h->params.debye_length;
   C.inv_xi2 = C.inv_xi * C.inv_xi;
   C.c_lj = (float)((double)h->params.lj_cf * (double)h->params.kbt_cf);
-  const int grid = std::min(h->n_items, h->num_sms * 8);
   const bool cut = h->params.crowder_cutoff > 0.0f;
   auto adj = h->params.crowder_mode ? (cut ? adjoint_tile_kernel<true, true>
                                            : adjoint_tile_kernel<true, false>)
                                     : (cut ? adjoint_tile_kernel<false, true>
                                            : adjoint_tile_kernel<false, false>);
+  // a persistent grid: as many CTAs as fit on the GPU at once
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj, kTile, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 8;
+  const int grid = std::min(h->n_items, h->num_sms * per_sm);
   adj<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab, h->d_mol_start,
                                      h->d_items, h->n_items, h->d_forces, h->d_G, h->d_dxi,
                                      h->d_eadj, consts_of(h), C);
   REMC_CUDA_TRY(cudaGetLastError());
-  molecule_force_torque_kernel<<<h->n_inst, 256, 0, h->stream>>>(
+  molecule_force_torque_kernel<<<dim3(h->n_inst, (h->mmax + 127) / 128), 128, 0, h->stream>>>(
       h->d_sys, h->d_inst_sys, h->d_mol_start, h->d_rel, h->d_forces, h->d_mft);
   REMC_CUDA_TRY(cudaGetLastError());
   if (forces)
