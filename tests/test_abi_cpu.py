@@ -91,3 +91,20 @@ def test_create_rejects_bad_descriptors_without_gpu(built_lib):
     rc = lib().remc_create(ctypes.byref(d), 1, ctypes.byref(p), ctypes.byref(h))
     assert rc == REMC_ERR_INVALID
     assert b"type" in lib().remc_last_error_string()
+
+
+@pytest.mark.parametrize("exe", ["REMCDockingGPU", "REMCDockingGPU_streams", "ref_gpu_check"])
+def test_reference_gpu_build_links_this_library(exe):
+    """The reference's own GPU build (its unmodified sources with -DEnableCUDA
+    and include/remc_cudaexterns.h force-included, made by oracle/build.py)
+    takes its GPU entry points from libremc_b200.so."""
+    import subprocess
+    path = os.path.join(ROOT, "oracle", "_ref", exe)
+    if not os.path.exists(path):
+        pytest.skip("the reference's GPU build is made where the reference tree is present")
+    out = subprocess.run(["readelf", "-d", path], capture_output=True, text=True).stdout
+    assert "libremc_b200.so" in out
+    syms = subprocess.run(["nm", "-D", "--undefined-only", path], capture_output=True,
+                          text=True).stdout
+    for name in ("CUDA_EonDevice", "copyLJPotentialDataToDevice", "CUDA_setBoxDimension"):
+        assert name in syms, name
