@@ -391,27 +391,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     cooperative_groups::this_cluster().sync();
   else
     __syncthreads();
-  // the next step's record fields, its molecule's centre and, for a
-  // one-bead molecule, its bead, loaded one step ahead (right after the
-  // previous step's barrier) so that a step starts without waiting on them.
-  // A molecule that the current step moves and accepts is taken from
-  // registers in the next step instead (same), so the early loads never
-  // need a value the current step writes.
-  int nx_m = 0, nx_m0 = 0, nx_info = 0;
-  float nx_t0 = 0.f, nx_t1 = 0.f, nx_t2 = 0.f;
-  float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f), next_b = next_c;
-  auto load_next = [&](int step) {
-    const StepRec& r = s_ring[step & (kRing - 1)];
-    nx_m = r.m;
-    nx_m0 = r.m0;
-    nx_info = r.info;
-    nx_t0 = r.t[0];
-    nx_t1 = r.t[1];
-    nx_t2 = r.t[2];
-    next_c = cent[nx_m];
-    if ((nx_info & kRecCount) == 1) next_b = s_beads[nx_m0];
-  };
-  if (n_steps > 0) load_next(0);
+  float4 next_c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (n_steps > 0 && !A.mol_in_smem) next_c = cent[s_ring[0].m];
 
   // previous step, known to every thread
   int p_m = -1, p_acc = 0, p_rot = 0, p_n = 0, p_b = 0;
@@ -437,15 +418,14 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       int m, rotate, crowd;
       float t[3];
     } rec;
-    rec.m = nx_m;
-    rec.rotate = (nx_info & kRecRotate) != 0;
-    rec.crowd = (nx_info & kRecCrowd) != 0;
-    rec.t[0] = nx_t0;
-    rec.t[1] = nx_t1;
-    rec.t[2] = nx_t2;
+    rec.m = recs_.m;
+    rec.rotate = (recs_.info & kRecRotate) != 0;
+    rec.crowd = (recs_.info & kRecCrowd) != 0;
+    rec.t[0] = recs_.t[0];
+    rec.t[1] = recs_.t[1];
+    rec.t[2] = recs_.t[2];
     const int m = rec.m;
-    const int m0 = nx_m0, n = nx_info & kRecCount;
-    const float4 this_b = next_b;
+    const int m0 = recs_.m0, n = recs_.info & kRecCount;
     const int b = s & 1;
     const bool same = (m == p_m) && p_acc;  // moved (and accepted) last step
     // centre of m: the one this step's thread computed last step if m moved
@@ -456,7 +436,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
       c1 = p_nc1;
       c2 = p_nc2;
     } else {
-      const float4 c = next_c;
+      const float4 c = A.mol_in_smem ? cent[m] : next_c;
       c0 = c.x;
       c1 = c.y;
       c2 = c.z;
@@ -483,7 +463,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     const bool skip = rec.rotate && n == 1;
     float4 pold1, pnew1;  // one-bead molecule: old/new position in registers
     if (n == 1) {
-      pold1 = same ? p_single : this_b;
+      pold1 = same ? p_single : s_beads[m0];
       pnew1 = make_float4(nc0, nc1, nc2, pold1.w);
     } else {
       // trial positions of the chain, built by the owners of its beads
@@ -737,11 +717,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
 
     // ---- every thread: the same FP64 sums (a fixed pairwise tree over the
     // warps' partials) and the same Metropolis decision
-    if (s + 1 < n_steps) {
-      // the next step's record, centre and bead, loaded while this step
-      // finishes; if that molecule moves in this step, the next step takes
-      // its centre and bead from registers instead (same)
-      load_next(s + 1);
+    if (s + 1 < n_steps && A.mol_in_smem == 0) {
+      next_c = cent[s_ring[(s + 1) & (kRing - 1)].m];
     }
     double dE = tree_sum8(s_red + b * csize * 64);
     double dE_cc = 0.0;
