@@ -1497,10 +1497,11 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
     const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
-    float* __restrict__ forces, double* __restrict__ G, double* __restrict__ dxi,
-    double* __restrict__ e_out, EnergyConsts K, AdjConsts C) {
+    int* __restrict__ queue, float* __restrict__ forces, double* __restrict__ G,
+    double* __restrict__ dxi, double* __restrict__ e_out, EnergyConsts K, AdjConsts C) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ float4 s_j[kTile];
+  __shared__ int s_it;  // the CTA's next item, from the work queue
   // the tile's crowder part [jc, jn) again, by coordinate, in groups of 8
   // from jc with beads q and q + 4 side by side: copy 0 in the order
   // (q, q + 4) for lanes 0-15, copy 1 in the order (q + 4, q) for lanes 16-31
@@ -1513,7 +1514,14 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
   __shared__ double s_red[kTile / 32][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+  // items come from a work queue over a list ordered by decreasing cost, so
+  // the CTAs finish together (the outputs are sums of atomics: any item
+  // order gives them)
+  if (tid == 0) s_it = atomicAdd(queue, 1);
+  for (;;) {
+    __syncthreads();  // the previous item is done with the shared buffers; s_it is set
+    const int it = s_it;
+    if (it >= n_items) break;
     const TileItem W = items[it];
     const SysDev S = sys[inst_sys[W.inst]];
     const int N = S.n_beads;
@@ -1522,7 +1530,6 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
     const int j0 = W.tj * kTile;
     const int jn = min(kTile, N - j0);
     const int jc = max(0, min(jn, S.n_chain_beads - j0));  // [0, jc) residues, [jc, jn) crowders
-    __syncthreads();  // the previous item is done with the shared buffers
     if (tid < jn) {
       const float4 p = pos[base + j0 + tid];
       s_j[tid] = p;
@@ -1629,6 +1636,7 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
       }
       atomicAdd(&e_out[W.inst], e);
       atomicAdd(&dxi[W.inst], x * (double)C.inv_xi2);
+      s_it = atomicAdd(queue, 1);  // every thread read s_it before this item's barriers
     }
   }
 }
@@ -1825,6 +1833,8 @@ struct remc_handle {
   int max_dyn_smem = 0;
   int config_gen = 0;  // bumped when the sweep schedule changes
   TileItem* d_items = nullptr;
+  TileItem* d_adj_items = nullptr;  // the adjoint's items, by decreasing cost
+  int* d_adj_queue = nullptr;
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
   double* d_scratch_cc = nullptr;
@@ -1884,7 +1894,8 @@ void free_all(remc_handle* h) {
                   h->d_queue,      h->d_scratch_cc, h->d_ecc,     h->d_n_samples,  h->d_n_bound,
                   h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_forces, h->d_G,
                   h->d_dxi,        h->d_eadj,     h->d_mft,
-                  h->d_ctrl,     h->d_items,     h->d_item_off,   h->d_scratch,    h->d_newpos,
+                  h->d_ctrl,     h->d_items,     h->d_adj_items,  h->d_adj_queue,
+                  h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad,
                   h->d_err,      h->d_trial_scratch, h->d_fold_part};
   for (void* p : ptrs)
@@ -2374,6 +2385,23 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   }
   item_off.push_back((int)items.size());
   h->n_items = (int)items.size();
+  // the adjoint's order: decreasing estimated cost (pairs, residue pairs
+  // weighted up), stable
+  std::vector<TileItem> adj_items(items);
+  {
+    auto cost = [&](const TileItem& W) {
+      const SysDev& S = h->h_sys[h->h_inst_sys[W.inst]];
+      const int N = S.n_beads, ncb = S.n_chain_beads;
+      const long long in = std::min(kTile, N - W.ti * kTile), jn = std::min(kTile, N - W.tj * kTile);
+      const long long ir = std::max(0, std::min((int)in, ncb - W.ti * kTile));
+      const long long jr = std::max(0, std::min((int)jn, ncb - W.tj * kTile));
+      const long long pairs = W.ti == W.tj ? in * (in - 1) / 2 : in * jn;
+      const long long rr = W.ti == W.tj ? ir * (ir - 1) / 2 : ir * jr;
+      return 2 * pairs + rr;
+    };
+    std::stable_sort(adj_items.begin(), adj_items.end(),
+                     [&](const TileItem& a, const TileItem& b) { return cost(a) > cost(b); });
+  }
   // ---- device memory
   int rc = REMC_OK;
   e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -2428,6 +2456,8 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_ctrl, 4);
   if (!rc) rc = dev_alloc(&h->d_queue, 1);
   if (!rc) rc = dev_alloc(&h->d_items, items.size());
+  if (!rc) rc = dev_alloc(&h->d_adj_items, items.size());
+  if (!rc) rc = dev_alloc(&h->d_adj_queue, 1);
   if (!rc) rc = dev_alloc(&h->d_item_off, item_off.size());
   if (!rc) rc = dev_alloc(&h->d_scratch, items.size());
   if (!rc) rc = dev_alloc(&h->d_scratch_cc, items.size());
@@ -2455,6 +2485,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   }
   up(h->d_mrole_off, mrole_off.data(), sizeof(int) * h->n_sys);
   up(h->d_items, items.data(), sizeof(TileItem) * items.size());
+  up(h->d_adj_items, adj_items.data(), sizeof(TileItem) * adj_items.size());
   up(h->d_item_off, item_off.data(), sizeof(int) * item_off.size());
   // per bead per instance: the meta word of pos.w, and bit 31 for beads of
   // one-bead molecules (whose relative position must be zero)
@@ -2912,6 +2943,7 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
                                 h->stream));
   REMC_CUDA_TRY(cudaMemsetAsync(h->d_dxi, 0, sizeof(double) * h->n_inst, h->stream));
   REMC_CUDA_TRY(cudaMemsetAsync(h->d_eadj, 0, sizeof(double) * h->n_inst, h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_adj_queue, 0, sizeof(int), h->stream));
   AdjConsts C;
   C.inv_xi = 1.0f / h->params.debye_length;
   C.inv_xi2 = C.inv_xi * C.inv_xi;
@@ -2928,8 +2960,8 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
     per_sm = 8;
   const int grid = std::min(h->n_items, h->num_sms * per_sm);
   adj<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab, h->d_mol_start,
-                                     h->d_items, h->n_items, h->d_forces, h->d_G, h->d_dxi,
-                                     h->d_eadj, consts_of(h), C);
+                                     h->d_adj_items, h->n_items, h->d_adj_queue, h->d_forces,
+                                     h->d_G, h->d_dxi, h->d_eadj, consts_of(h), C);
   REMC_CUDA_TRY(cudaGetLastError());
   molecule_force_torque_kernel<<<dim3(h->n_inst, (h->mmax + 127) / 128), 128, 0, h->stream>>>(
       h->d_sys, h->d_inst_sys, h->d_mol_start, h->d_rel, h->d_forces, h->d_mft);
