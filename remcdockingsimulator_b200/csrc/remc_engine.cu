@@ -399,11 +399,6 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   float4 p_single = make_float4(0.f, 0.f, 0.f, 0.f);  // accepted one-bead position
   float p_nc0 = 0.f, p_nc1 = 0.f, p_nc2 = 0.f;          // accepted new centre
 
-  // a crowder of the system's one species: its table row and its entry
-  // against crowders are the same at every step; so is the packed box
-  const float4* const trow_c = s_tab + (ctype >= 0 ? ctype : 0) * kNT;
-  const float4 Tcc = trow_c[ctype >= 0 ? ctype : 0];
-  const PackedBox PBi = packed_box(box, invbox);
   for (int s = 0; s < n_steps; ++s) {
     // ---- prefetch the next ring half (records s+31 .. s+62). The half it
     // overwrites ends with step s-2's record, which is read until after step
@@ -514,12 +509,10 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           // sum), two j per pass with both loads issued first, the moved
           // bead itself (j = m0) left out of the sum
           const bool one_ct = ctype >= 0;
-          // with one crowder species the moved crowder's row is trow_c
-          const float4* const trw = one_ct ? trow_c : trow;
-          const float4 Tc = Tcc;  // used only with one species
+          const float4 Tc = trow[one_ct ? ctype : 0];
           // the two beads of a pass as the two lanes of packed FP32, against
           // the moved bead's new and old position (negated once per step)
-          const PackedBox& PB1 = PBi;
+          const PackedBox PB1 = packed_box(box, invbox);
           const float2 nnx = make_float2(-pnew1.x, -pnew1.x), nny = make_float2(-pnew1.y, -pnew1.y),
                        nnz = make_float2(-pnew1.z, -pnew1.z);
           const float2 nox = make_float2(-pold1.x, -pold1.x), noy = make_float2(-pold1.y, -pold1.y),
@@ -531,8 +524,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             for (; j + gstride < N; j += 2 * gstride) {
               const int j2 = j + gstride;
               const float4 pa = s_beads[j], pb = s_beads[j2];
-              const float4 Ta = (one_ct && j >= ncb) ? Tc : trw[bead_type(pa.w)];
-              const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trw[bead_type(pb.w)];
+              const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
+              const float4 Tb = (one_ct && j2 >= ncb) ? Tc : trow[bead_type(pb.w)];
               const float2 xj = make_float2(pa.x, pb.x), yj = make_float2(pa.y, pb.y),
                            zj = make_float2(pa.z, pb.z);
               const float2 A2 = make_float2(Ta.x, Tb.x), C2 = make_float2(Ta.z, Tb.z);
@@ -548,7 +541,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           if (S.fold_mi) pass1(std::true_type{}); else pass1(std::false_type{});
           if (j < N && j != m0) {
             const float4 pa = s_beads[j];
-            const float4 Ta = (one_ct && j >= ncb) ? Tc : trw[bead_type(pa.w)];
+            const float4 Ta = (one_ct && j >= ncb) ? Tc : trow[bead_type(pa.w)];
             const float en = crowd_energy<R12, CUT>(pair_r2(pnew1, pa, box, invbox), Ta.x, Ta.z);
             const float eo = crowd_energy<R12, CUT>(pair_r2(pold1, pa, box, invbox), Ta.x, Ta.z);
             acc_o += en - eo;
@@ -592,7 +585,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
           if (!rec.crowd) {
             // residue pairs: the new and the old evaluation of a pair as the
             // two lanes of packed FP32
-            const PackedBox& PB = PBi;
+            const PackedBox PB = packed_box(box, invbox);
             auto pass2 = [&](auto fold) {
               constexpr bool F = decltype(fold)::value;
               for (; j + gstride < cb; j += 2 * gstride) {
@@ -650,7 +643,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
             }
           }
           const bool one_ct = ctype >= 0;
-          const PackedBox& PBc = PBi;
+          const PackedBox PBc = packed_box(box, invbox);
           auto pass3 = [&](auto fold) {
             constexpr bool F = decltype(fold)::value;
             for (; j + gstride < hi; j += 2 * gstride) {
