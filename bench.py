@@ -437,8 +437,9 @@ def main():
         cpu = cpu_baseline(w, args.seed)
 
     # per timed step: ctrl_set_kernel (remc_run) + the graph's proposal_kernel,
-    # sweep_kernel, exchange_kernel and ctrl_advance_kernel
-    gpu_launches = args.steps * 5
+    # block_cost_kernel and rank_kernel (work order by proposal cost, single
+    # CTAs per replica), sweep_kernel, exchange_kernel and ctrl_advance_kernel
+    gpu_launches = args.steps * (3 + eng.work_order()[1])
     if rank == 0:
         line = {
             "metric": "REMC replica-steps/s (batched persistent sweep + CUDA graph)",

@@ -242,6 +242,18 @@ int remc_set_bead_storage(remc_handle* h, int in_shared_memory);
  * rounding. No reference counterpart. */
 int remc_get_fold_flags(remc_handle* h, int* per_system);
 int remc_get_bead_storage(remc_handle* h, int* in_shared_memory);
+/* Work order of the persistent sweep (single CTAs per replica). 1 (the
+ * default): before each launch, a kernel sums what every replica's proposals
+ * for the block cost (the pair evaluations of each step's moved molecule plus
+ * a per-step allowance) and a second ranks the replicas, so the work queue
+ * hands out the most expensive blocks first and the slots finish together.
+ * 0: the static order fixed at remc_create (by each system's expected cost
+ * per step). Results are identical either way: every replica's trajectory is
+ * independent of when it runs. launches_per_sweep (may be NULL): kernels per
+ * sweep launch, 4 with the cost order (proposals, cost, rank, sweep), else 2.
+ * No reference counterpart. */
+int remc_set_work_order(remc_handle* h, int by_cost);
+int remc_get_work_order(remc_handle* h, int* by_cost, int* launches_per_sweep);
 
 int remc_sync(remc_handle* h);
 /* Failure-path check: runs one warp whose bounded device-side wait (the one

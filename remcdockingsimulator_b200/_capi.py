@@ -94,6 +94,8 @@ _SIGS = {
     "remc_set_schedule": (C.c_int, [P, C.c_int, C.c_int]),
     "remc_set_cluster": (C.c_int, [P, C.c_int]),
     "remc_get_schedule": (C.c_int, [P, PI, PI, PI]),
+    "remc_set_work_order": (C.c_int, [P, C.c_int]),
+    "remc_get_work_order": (C.c_int, [P, PI, PI]),
     "remc_set_bead_storage": (C.c_int, [P, C.c_int]),
     "remc_get_bead_storage": (C.c_int, [P, PI]),
     "remc_check_wait_timeout": (C.c_int, [P, C.c_int]),

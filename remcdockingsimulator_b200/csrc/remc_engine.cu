@@ -160,6 +160,62 @@ __global__ void __launch_bounds__(256) proposal_kernel(ProposalArgs P) {
   P.recs[(size_t)inst * P.rec_stride + s] = r;
 }
 
+// Work order of the persistent sweep. Its makespan is set by the replicas that
+// take longest, and a replica's block of steps costs what its proposals ask
+// for: which molecules move (a chain of n beads against the other N - n
+// beads, or one bead) is drawn before the sweep. block_cost_kernel sums, per
+// instance, the pair evaluations of its n_steps records plus `step_cost` per
+// step for the step's fixed work (record, reduction, barrier, decision); a
+// one-bead rotation has no pairs. Integer sums, so the result does not depend
+// on the order of the additions. One CTA per instance.
+__global__ void __launch_bounds__(256) block_cost_kernel(const SysDev* __restrict__ sys,
+                                                         const int* __restrict__ inst_sys,
+                                                         const StepRec* __restrict__ recs,
+                                                         int rec_stride, int n_steps,
+                                                         long long step_cost,
+                                                         long long* __restrict__ cost) {
+  const int inst = blockIdx.x;
+  const int N = sys[inst_sys[inst]].n_beads;
+  const StepRec* r = recs + (size_t)inst * rec_stride;
+  long long c = 0;
+  for (int s = threadIdx.x; s < n_steps; s += blockDim.x) {
+    const int info = r[s].info;
+    const long long n = info & kRecCount;
+    const bool still = (info & kRecRotate) && n == 1;  // a one-bead rotation moves nothing
+    c += (still ? 0 : n * (N - n)) + step_cost;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  __shared__ unsigned long long s_sum;
+  if (threadIdx.x == 0) s_sum = 0ull;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) atomicAdd(&s_sum, (unsigned long long)c);
+  __syncthreads();
+  if (threadIdx.x == 0) cost[inst] = (long long)s_sum;
+}
+
+// order[k] = the instance of rank k by decreasing cost, ties by instance
+// index: a strict total order, so the ranks are a permutation. O(n^2)
+// comparisons through shared-memory tiles (n up to kMaxRankedInst).
+constexpr int kMaxRankedInst = 65536;
+__global__ void __launch_bounds__(256) rank_kernel(const long long* __restrict__ cost, int n,
+                                                   int* __restrict__ order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ci = i < n ? cost[i] : 0;
+  int rank = 0;
+  __shared__ long long s_c[256];
+  for (int base = 0; base < n; base += 256) {
+    __syncthreads();
+    if (base + (int)threadIdx.x < n) s_c[threadIdx.x] = cost[base + threadIdx.x];
+    __syncthreads();
+    const int m = min(256, n - base);
+    for (int k = 0; k < m; ++k) {
+      const long long cj = s_c[k];
+      rank += (cj > ci) || (cj == ci && base + k < i);
+    }
+  }
+  if (i < n) order[rank] = i;
+}
+
 // A bound conformation recorded by Replica::sample (Replica.cpp:1717-1780):
 // header + one pose (rotation quaternion, centre) per molecule.
 struct SampleHeader {
@@ -1798,6 +1854,9 @@ struct remc_handle {
   SysDev* d_sys = nullptr;
   int* d_inst_sys = nullptr;
   int* d_inst_list = nullptr;
+  long long* d_inst_cost = nullptr;  // per instance: cost of the current block of steps
+  int* d_inst_order = nullptr;       // work order of the persistent sweep, by that cost
+  int work_order = 1;                // 1: by the block's proposal costs; 0: static order
   float4* d_pos = nullptr;
   float4* d_rel = nullptr;
   float4* d_centre = nullptr;
@@ -1888,7 +1947,8 @@ int dev_alloc(T** p, size_t n) {
 }
 
 void free_all(remc_handle* h) {
-  void* ptrs[] = {h->d_sys,      h->d_inst_sys,  h->d_inst_list,  h->d_pos,        h->d_rel,
+  void* ptrs[] = {h->d_sys,      h->d_inst_sys,  h->d_inst_list,  h->d_inst_cost,  h->d_inst_order,
+                  h->d_pos,        h->d_rel,
                   h->d_centre,   h->d_quat,      h->d_mol_start,  h->d_tab,        h->d_energy,
                   h->d_temp_idx, h->d_slot_of_temp, h->d_ladder,  h->d_tstep,      h->d_rot_cs,
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
@@ -2191,13 +2251,38 @@ int launch_sweep_kernel(remc_handle* h, int n_steps, int rec_offset, const int* 
   return REMC_OK;
 }
 
+// A step's fixed work (record, reductions, barrier, decision) in pair
+// evaluations, per thread of the replica: about 1,500 pair evaluations at 256
+// threads, from per-step clock64 timings of one-bead and chain steps on the
+// 64-system batch (a step costs about 1,700 cycles plus 1.1 per pair there).
+constexpr long long kStepCostPerThread = 6;
+
+// The persistent sweep takes its work in cost order (remc_set_work_order).
+bool uses_cost_order(const remc_handle* h) {
+  return h->work_order == 1 && h->sweep_csize == 1 && h->n_inst > 1 &&
+         h->n_inst <= kMaxRankedInst;
+}
+
 // Proposals then one persistent sweep over all instances, for n_steps steps
 // (the record buffer must already hold n_steps records per instance).
 int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
                  const uint32_t* ctrl) {
   int rc = launch_proposals(h, n_steps, seed, step0, ctrl);
   if (rc) return rc;
-  return launch_sweep_kernel(h, n_steps, 0, h->d_inst_list, h->n_inst, true, step0, ctrl);
+  // the work queue in decreasing order of what each replica's proposals cost
+  // (single CTAs per replica: a cluster schedule runs every replica at once)
+  const int* list = h->d_inst_list;
+  if (uses_cost_order(h) && n_steps > 0) {
+    block_cost_kernel<<<h->n_inst, 256, 0, h->stream>>>(
+        h->d_sys, h->d_inst_sys, h->d_recs, (int)h->recs_cap, n_steps,
+        kStepCostPerThread * (long long)h->sweep_threads, h->d_inst_cost);
+    REMC_CUDA_TRY(cudaGetLastError());
+    rank_kernel<<<(h->n_inst + 255) / 256, 256, 0, h->stream>>>(h->d_inst_cost, h->n_inst,
+                                                                 h->d_inst_order);
+    REMC_CUDA_TRY(cudaGetLastError());
+    list = h->d_inst_order;
+  }
+  return launch_sweep_kernel(h, n_steps, 0, list, h->n_inst, true, step0, ctrl);
 }
 
 }  // namespace
@@ -2429,6 +2514,8 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_sys, h->h_sys.size());
   if (!rc) rc = dev_alloc(&h->d_inst_sys, h->n_inst);
   if (!rc) rc = dev_alloc(&h->d_inst_list, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_inst_cost, h->n_inst);
+  if (!rc) rc = dev_alloc(&h->d_inst_order, h->n_inst);
   if (!rc) rc = dev_alloc(&h->d_pos, h->total_beads);
   if (!rc) rc = dev_alloc(&h->d_bead_info, h->total_beads);
   if (!rc) rc = dev_alloc(&h->d_stage, 6 * h->total_beads + 3 * h->total_mols);
@@ -3235,6 +3322,22 @@ int remc_set_bead_storage(remc_handle* h, int in_shared_memory) {
   REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return configure_sweep(h, h->sweep_threads, h->mol_in_smem, h->sweep_csize,
                          in_shared_memory ? 1 : 0);
+}
+
+int remc_set_work_order(remc_handle* h, int by_cost) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (by_cost != 0 && by_cost != 1) return set_error(REMC_ERR_INVALID, "work order must be 0 or 1");
+  REMC_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->work_order = by_cost;
+  h->config_gen++;  // captured graphs hold the launch sequence
+  return REMC_OK;
+}
+
+int remc_get_work_order(remc_handle* h, int* by_cost, int* launches_per_sweep) {
+  if (!h) return set_error(REMC_ERR_INVALID, "null handle");
+  if (by_cost) *by_cost = h->work_order;
+  if (launches_per_sweep) *launches_per_sweep = uses_cost_order(h) ? 4 : 2;
+  return REMC_OK;
 }
 
 int remc_get_bead_storage(remc_handle* h, int* in_shared_memory) {

@@ -368,6 +368,17 @@ class Engine:
         check(lib().remc_get_schedule(self._h, C.byref(t), C.byref(m), C.byref(c)))
         return t.value, bool(m.value), c.value
 
+    def set_work_order(self, by_cost: bool) -> None:
+        """Persistent sweep work order: by each block's proposal costs (True,
+        the default) or the static order (False); results are identical."""
+        check(lib().remc_set_work_order(self._h, 1 if by_cost else 0))
+
+    def work_order(self):
+        """(by cost, kernel launches per sweep launch)."""
+        b, n = C.c_int(), C.c_int()
+        check(lib().remc_get_work_order(self._h, C.byref(b), C.byref(n)))
+        return bool(b.value), n.value
+
     def set_schedule(self, threads: int, mol_in_smem: bool) -> None:
         check(lib().remc_set_schedule(self._h, threads, 1 if mol_in_smem else 0))
 

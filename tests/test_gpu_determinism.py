@@ -75,3 +75,27 @@ def test_batch64_runs_are_bit_identical(built_lib):
     w = synth.batch64(0)
     runs = {_run(w.systems, w.n_replicas, w.ladders, w.params, 3000) for _ in range(2)}
     assert len(runs) == 1, runs
+
+
+def test_work_order_does_not_change_results(built_lib):
+    """The persistent sweep takes replicas in decreasing order of their block's
+    proposal costs (block_cost_kernel + rank_kernel before every launch), or in
+    the static order: every replica's trajectory is the same either way. A
+    rank that was not a permutation would run some replica twice and another
+    not at all."""
+    from remcdockingsimulator_b200 import synth
+    from remcdockingsimulator_b200.engine import Engine
+    w = synth.batch64(0)
+    digests = []
+    for by_cost in (True, False):
+        with Engine(w.systems, w.n_replicas, w.params) as eng:
+            eng.set_replica_params(w.ladders, np.full(len(w.systems), 1.0, np.float32),
+                                   np.full(len(w.systems), 0.4))
+            eng.set_work_order(by_cost)
+            assert eng.work_order() == (by_cost, 4 if by_cost else 2)
+            eng.energy_full()
+            for k in range(0, 2000, 1000):
+                eng.sweep(1000, 4242, k)
+            eng.run(2, 500, 4242, 2000, 0)
+            digests.append(_digest(eng))
+    assert digests[0] == digests[1]
