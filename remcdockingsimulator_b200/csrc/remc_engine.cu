@@ -194,26 +194,22 @@ __global__ void __launch_bounds__(256) block_cost_kernel(const SysDev* __restric
 }
 
 // order[k] = the instance of rank k by decreasing cost, ties by instance
-// index: a strict total order, so the ranks are a permutation. O(n^2)
-// comparisons through shared-memory tiles (n up to kMaxRankedInst).
+// index: a strict total order, so the ranks are a permutation. One warp per
+// instance; its lanes split the n comparisons (n up to kMaxRankedInst).
 constexpr int kMaxRankedInst = 65536;
 __global__ void __launch_bounds__(256) rank_kernel(const long long* __restrict__ cost, int n,
                                                    int* __restrict__ order) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const long long ci = i < n ? cost[i] : 0;
-  int rank = 0;
-  __shared__ long long s_c[256];
-  for (int base = 0; base < n; base += 256) {
-    __syncthreads();
-    if (base + (int)threadIdx.x < n) s_c[threadIdx.x] = cost[base + threadIdx.x];
-    __syncthreads();
-    const int m = min(256, n - base);
-    for (int k = 0; k < m; ++k) {
-      const long long cj = s_c[k];
-      rank += (cj > ci) || (cj == ci && base + k < i);
-    }
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;  // whole warps
+  const long long ci = cost[i];
+  unsigned rank = 0;
+  for (int j = lane; j < n; j += 32) {
+    const long long cj = cost[j];
+    rank += (cj > ci) || (cj == ci && j < i);
   }
-  if (i < n) order[rank] = i;
+  rank = __reduce_add_sync(0xffffffffu, rank);
+  if (lane == 0) order[rank] = i;
 }
 
 // A bound conformation recorded by Replica::sample (Replica.cpp:1717-1780):
@@ -2277,8 +2273,8 @@ int launch_sweep(remc_handle* h, int n_steps, uint64_t seed, uint32_t step0,
         h->d_sys, h->d_inst_sys, h->d_recs, (int)h->recs_cap, n_steps,
         kStepCostPerThread * (long long)h->sweep_threads, h->d_inst_cost);
     REMC_CUDA_TRY(cudaGetLastError());
-    rank_kernel<<<(h->n_inst + 255) / 256, 256, 0, h->stream>>>(h->d_inst_cost, h->n_inst,
-                                                                 h->d_inst_order);
+    rank_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(h->d_inst_cost, h->n_inst,
+                                                             h->d_inst_order);
     REMC_CUDA_TRY(cudaGetLastError());
     list = h->d_inst_order;
   }
