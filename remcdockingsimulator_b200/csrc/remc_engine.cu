@@ -1051,7 +1051,8 @@ __global__ void fold_flag_kernel(SysDev* __restrict__ sys, const float* __restri
 
 // ------------------------------------------------------------------ full E
 struct TileItem {
-  int inst, ti, tj, pad;
+  int inst, ti, tj;
+  int slot;  // the item's place in the instance-grouped list (its partial's slot)
 };
 
 constexpr int kTile = 128;
@@ -1190,8 +1191,8 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
     const SysDev* __restrict__ sys, const int* __restrict__ inst_sys,
     const float4* __restrict__ pos, const float4* __restrict__ tab,
     const int* __restrict__ mol_start, const TileItem* __restrict__ items, int n_items,
-    double* __restrict__ scratch, double* __restrict__ scratch_cc, EnergyConsts K,
-    int* __restrict__ err) {
+    int* __restrict__ queue, double* __restrict__ scratch, double* __restrict__ scratch_cc,
+    EnergyConsts K, int* __restrict__ err) {
   __shared__ float4 s_tab[kNT * kNT];
   __shared__ __align__(128) float4 s_j[2][kTile];  // two stages
   // the tile by coordinate, and its bead types, per stage
@@ -1200,22 +1201,33 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
   __shared__ double s_red[2][kTile / 32];
   __shared__ double s_red_cc[2][kTile / 32];
   __shared__ __align__(8) unsigned long long s_bar[2];
+  // the items whose tiles are (or go next) in buffers 0 and 1, from a work
+  // queue over the list sorted by decreasing cost; each item's partials go
+  // to its slot in the instance-grouped list, so the per-instance reduction
+  // does not depend on which CTA took which item, or when
+  __shared__ int s_item[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kNT * kNT; i += kTile) s_tab[i] = tab[i];
   if (tid == 0) {
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
-    if ((int)blockIdx.x < n_items) {
+    const int first = atomicAdd(queue, 1);
+    s_item[0] = first;
+    s_item[1] = atomicAdd(queue, 1);
+    if (first < n_items) {
       unsigned bytes;
-      const float4* src = tile_src(sys, inst_sys, pos, items[blockIdx.x], &bytes);
+      const float4* src = tile_src(sys, inst_sys, pos, items[first], &bytes);
       bulk_load(s_j[0], src, bytes, &s_bar[0]);
     }
   }
-  __syncthreads();  // barriers initialised
+  __syncthreads();  // barriers initialised, s_item set
   unsigned phases = 0;  // bit b: parity of buffer b's next completion
   int buf = 0;
-  int prev = -1;  // the previous item, whose partials thread 0 writes out
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x, buf ^= 1) {
+  int prev = -1;  // the previous item's slot, whose partials thread 0 writes out
+  for (;; buf ^= 1) {
+    // s_item[buf] was written before a barrier every thread has passed
+    const int it = s_item[buf];
+    if (it >= n_items) break;
     const TileItem W = items[it];
     const SysDev S = sys[inst_sys[W.inst]];
     const int N = S.n_beads;
@@ -1256,8 +1268,8 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
       }
       return;
     }
-    const int next = it + (int)gridDim.x;
     if (tid == 0) {
+      const int next = s_item[buf ^ 1];  // written by this thread
       if (prev >= 0) {
         double v = 0.0, c = 0.0;
         for (int w = 0; w < kTile / 32; ++w) {
@@ -1272,6 +1284,9 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
         const float4* src = tile_src(sys, inst_sys, pos, items[next], &bytes);
         bulk_load(s_j[buf ^ 1], src, bytes, &s_bar[buf ^ 1]);
       }
+      // the item after next, for this buffer: every thread read s_item[buf]
+      // before this item's barrier
+      s_item[buf] = atomicAdd(queue, 1);
     }
     double dsum = 0.0, dcc = 0.0;
     if (ivalid) {
@@ -1305,7 +1320,7 @@ __global__ void __launch_bounds__(kTile) energy_tile_kernel(
       s_red[buf][warp] = dsum;
       s_red_cc[buf][warp] = dcc;
     }
-    prev = it;
+    prev = W.slot;
   }
   __syncthreads();  // the last item's partials are written
   if (tid == 0 && prev >= 0) {
@@ -1475,12 +1490,17 @@ __device__ __forceinline__ void adjoint_group(
 // coordinate. Works with e = p_j - p_i = -d: the forces it sums are the
 // negated pair forces (the caller negates the i-force sums; the j beads
 // receive them as they are).
-template <bool R12, bool CUT>
+// MASK: a group with pairs to leave out (j <= i in a diagonal tile, the i
+// bead's own molecule, j past the tile's end; coordinates there may be stale):
+// every pair is evaluated and the left-out ones' energy and forces are
+// replaced by zero, which costs less than the scalar checked path.
+template <bool R12, bool CUT, bool MASK>
 __device__ __forceinline__ void adjoint_group_crowd2(
     const float* __restrict__ gx8, const float* __restrict__ gy8,
     const float* __restrict__ gz8, float (*__restrict__ s_fjw)[3], int jg, int jend,
     float2 npx, float2 npy, float2 npz, float A, float cut2, float box, float invbox, int lane,
-    float2& nfx, float2& nfy, float2& nfz, float2& acc_e2) {
+    float2& nfx, float2& nfy, float2& nfz, float2& acc_e2, bool ivalid = true, int jlo = 0,
+    int ex0 = 0, int ex1 = 0) {
   const int r = (lane >> 2) & 7;
   const float kMagic = 12582912.0f;  // 1.5 * 2^23, as in min_image
   const float2 iL = make_float2(invbox, invbox), nL = make_float2(-box, -box);
@@ -1508,9 +1528,22 @@ __device__ __forceinline__ void adjoint_group_crowd2(
       e.x = (r2.x < cut2) ? e.x : 0.0f;
       e.y = (r2.y < cut2) ? e.y : 0.0f;
     }
+    bool va = true, vb = true;
+    if (MASK) {
+      const int ja = jg + (q ^ r), jb = jg + ((q + 4) ^ r);
+      va = ivalid && ja < jend && ja >= jlo && (unsigned)(ja - ex0) >= (unsigned)(ex1 - ex0);
+      vb = ivalid && jb < jend && jb >= jlo && (unsigned)(jb - ex0) >= (unsigned)(ex1 - ex0);
+      e.x = va ? e.x : 0.0f;
+      e.y = vb ? e.y : 0.0f;
+    }
     acc_e2 = __fadd2_rn(acc_e2, e);
     const float2 f = __fmul2_rn(__fmul2_rn(cf, e), rinv2);  // -(de/dr)/r
-    const float2 gx = __fmul2_rn(f, ex), gy = __fmul2_rn(f, ey), gz = __fmul2_rn(f, ez);
+    float2 gx = __fmul2_rn(f, ex), gy = __fmul2_rn(f, ey), gz = __fmul2_rn(f, ez);
+    if (MASK) {  // e = 0 can still meet rinv2 = inf (j = i, or stale coordinates)
+      gx = make_float2(va ? gx.x : 0.0f, vb ? gx.y : 0.0f);
+      gy = make_float2(va ? gy.x : 0.0f, vb ? gy.y : 0.0f);
+      gz = make_float2(va ? gz.x : 0.0f, vb ? gz.y : 0.0f);
+    }
     nfx = __fadd2_rn(nfx, gx);
     nfy = __fadd2_rn(nfy, gy);
     nfz = __fadd2_rn(nfz, gz);
@@ -1636,22 +1669,29 @@ __global__ void __launch_bounds__(kTile, 8) adjoint_tile_kernel(
                                             ex1, ivalid, pi, ta, a_crowd, Tc, tc_fixed, box,  \
                                             invbox, K, C, lane, fx, fy, fz, acc_e, acc_x);    \
   }
-    for (int jg = 0; jg < jc; jg += 8) REMC_ADJ_GROUP(true, jc)  // uniform trip counts
+    // in a diagonal tile every lane of warp w takes j > i >= 32 w: groups
+    // wholly below that add nothing and are left out (warp-uniform starts,
+    // group alignment kept: from 0 for residues, from jc for crowders)
+    const int jmin = (W.ti == W.tj) ? 32 * warp + 1 : 0;
+    const int jg_chain = (jmin >> 3) << 3;
+    const int jg_crowd = jc + (jmin > jc ? ((jmin - jc) >> 3) << 3 : 0);
+    for (int jg = jg_chain; jg < jc; jg += 8) REMC_ADJ_GROUP(true, jc)  // uniform trip counts
     if (tc_fixed) {
-      for (int jg = jc; jg < jn; jg += 8) {
+      for (int jg = jg_crowd; jg < jn; jg += 8) {
         const bool clean = ivalid && jg + 8 <= jn && jg >= jlo && (ex1 <= jg || ex0 >= jg + 8);
         if (__all_sync(0xffffffffu, clean))
-          adjoint_group_crowd2<R12, CUT>(s_px[half] + (jg - jc), s_py[half] + (jg - jc),
-                                         s_pz[half] + (jg - jc), s_fj[warp], jg, jn, npx, npy,
-                                         npz, Tc.x, Tc.z, box, invbox, lane, nfx, nfy, nfz,
-                                         acc_e2);
+          adjoint_group_crowd2<R12, CUT, false>(s_px[half] + (jg - jc), s_py[half] + (jg - jc),
+                                                s_pz[half] + (jg - jc), s_fj[warp], jg, jn, npx,
+                                                npy, npz, Tc.x, Tc.z, box, invbox, lane, nfx, nfy,
+                                                nfz, acc_e2);
         else
-          adjoint_group<R12, CUT, false, true>(s_j, s_tab, s_G, s_fj[warp], jg, jn, jlo, ex0, ex1,
-                                               ivalid, pi, ta, a_crowd, Tc, tc_fixed, box, invbox,
-                                               K, C, lane, fx, fy, fz, acc_e, acc_x);
+          adjoint_group_crowd2<R12, CUT, true>(s_px[half] + (jg - jc), s_py[half] + (jg - jc),
+                                               s_pz[half] + (jg - jc), s_fj[warp], jg, jn, npx,
+                                               npy, npz, Tc.x, Tc.z, box, invbox, lane, nfx, nfy,
+                                               nfz, acc_e2, ivalid, jlo, ex0, ex1);
       }
     } else {
-      for (int jg = jc; jg < jn; jg += 8) REMC_ADJ_GROUP(false, jn)
+      for (int jg = jg_crowd; jg < jn; jg += 8) REMC_ADJ_GROUP(false, jn)
     }
 #undef REMC_ADJ_GROUP
     fx -= nfx.x + nfx.y;
@@ -1889,13 +1929,17 @@ struct remc_handle {
   size_t trial_scratch_cap = 0;       // float4 entries
   int max_dyn_smem = 0;
   int config_gen = 0;  // bumped when the sweep schedule changes
-  TileItem* d_items = nullptr;
-  TileItem* d_adj_items = nullptr;  // the adjoint's items, by decreasing cost
-  int* d_adj_queue = nullptr;
+  TileItem* d_items_by_cost = nullptr;  // the items by decreasing cost (work-queue order)
+  int* d_adj_queue = nullptr;  // in d_adj_acc
+  int* d_energy_queue = nullptr;
   int* d_item_off = nullptr;
   double* d_scratch = nullptr;
   double* d_scratch_cc = nullptr;
-  float* d_forces = nullptr;   // adjoint outputs (allocated on first use)
+  // adjoint accumulators, one allocation (made on first use) so that one
+  // memset clears them all: forces, G, dxi, energy and the work counter
+  unsigned char* d_adj_acc = nullptr;
+  size_t adj_acc_bytes = 0;
+  float* d_forces = nullptr;
   double* d_G = nullptr;
   double* d_dxi = nullptr;
   double* d_eadj = nullptr;
@@ -1950,9 +1994,9 @@ void free_all(remc_handle* h) {
                   h->d_acc_neg,  h->d_acc_boltz, h->d_rej,        h->d_ex_tests,   h->d_ex_acc,
                   h->d_evals_kh, h->d_evals_crowd, h->d_mol_role, h->d_mrole_off, h->d_recs,
                   h->d_queue,      h->d_scratch_cc, h->d_ecc,     h->d_n_samples,  h->d_n_bound,
-                  h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_forces, h->d_G,
-                  h->d_dxi,        h->d_eadj,     h->d_mft,
-                  h->d_ctrl,     h->d_items,     h->d_adj_items,  h->d_adj_queue,
+                  h->d_sample_out, h->d_pose_out, h->d_sample_cursor, h->d_adj_acc,
+                  h->d_mft,
+                  h->d_ctrl,     h->d_items_by_cost, h->d_energy_queue,
                   h->d_item_off,   h->d_scratch,    h->d_newpos,
                   h->d_dE,       h->d_bead_info, h->d_stage,      h->d_stage_q,    h->d_bad,
                   h->d_err,      h->d_trial_scratch, h->d_fold_part};
@@ -2464,13 +2508,13 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     const SysDev& S = h->h_sys[h->h_inst_sys[g]];
     int nt = (S.n_beads + kTile - 1) / kTile;
     for (int ti = 0; ti < nt; ++ti)
-      for (int tj = ti; tj < nt; ++tj) items.push_back(TileItem{g, ti, tj, 0});
+      for (int tj = ti; tj < nt; ++tj) items.push_back(TileItem{g, ti, tj, (int)items.size()});
   }
   item_off.push_back((int)items.size());
   h->n_items = (int)items.size();
-  // the adjoint's order: decreasing estimated cost (pairs, residue pairs
-  // weighted up), stable
-  std::vector<TileItem> adj_items(items);
+  // the order of the energy and adjoint work queues: decreasing estimated
+  // cost (pairs, residue pairs weighted up), stable
+  std::vector<TileItem> items_by_cost(items);
   {
     auto cost = [&](const TileItem& W) {
       const SysDev& S = h->h_sys[h->h_inst_sys[W.inst]];
@@ -2482,7 +2526,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
       const long long rr = W.ti == W.tj ? ir * (ir - 1) / 2 : ir * jr;
       return 2 * pairs + rr;
     };
-    std::stable_sort(adj_items.begin(), adj_items.end(),
+    std::stable_sort(items_by_cost.begin(), items_by_cost.end(),
                      [&](const TileItem& a, const TileItem& b) { return cost(a) > cost(b); });
   }
   // ---- device memory
@@ -2540,9 +2584,8 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
   if (!rc) rc = dev_alloc(&h->d_ex_acc, h->n_sys);
   if (!rc) rc = dev_alloc(&h->d_ctrl, 4);
   if (!rc) rc = dev_alloc(&h->d_queue, 1);
-  if (!rc) rc = dev_alloc(&h->d_items, items.size());
-  if (!rc) rc = dev_alloc(&h->d_adj_items, items.size());
-  if (!rc) rc = dev_alloc(&h->d_adj_queue, 1);
+  if (!rc) rc = dev_alloc(&h->d_items_by_cost, items.size());
+  if (!rc) rc = dev_alloc(&h->d_energy_queue, 1);
   if (!rc) rc = dev_alloc(&h->d_item_off, item_off.size());
   if (!rc) rc = dev_alloc(&h->d_scratch, items.size());
   if (!rc) rc = dev_alloc(&h->d_scratch_cc, items.size());
@@ -2569,8 +2612,7 @@ int remc_create(const remc_system_desc* systems, int n_systems, const remc_param
     off += h->h_sys[s2].n_mol;
   }
   up(h->d_mrole_off, mrole_off.data(), sizeof(int) * h->n_sys);
-  up(h->d_items, items.data(), sizeof(TileItem) * items.size());
-  up(h->d_adj_items, adj_items.data(), sizeof(TileItem) * adj_items.size());
+  up(h->d_items_by_cost, items_by_cost.data(), sizeof(TileItem) * items_by_cost.size());
   up(h->d_item_off, item_off.data(), sizeof(int) * item_off.size());
   // per bead per instance: the meta word of pos.w, and bit 31 for beads of
   // one-bead molecules (whose relative position must be zero)
@@ -2770,10 +2812,10 @@ int remc_energy_full(remc_handle* h, double* out) {
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   int grid = std::min(h->n_items, h->num_sms * 8);
-  energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab,
-                                                   h->d_mol_start, h->d_items, h->n_items,
-                                                   h->d_scratch, h->d_scratch_cc, consts_of(h),
-                                                   h->d_err);
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_energy_queue, 0, sizeof(int), h->stream));
+  energy_tile_kernel<<<grid, kTile, 0, h->stream>>>(
+      h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab, h->d_mol_start, h->d_items_by_cost,
+      h->n_items, h->d_energy_queue, h->d_scratch, h->d_scratch_cc, consts_of(h), h->d_err);
   REMC_CUDA_TRY(cudaGetLastError());
   energy_reduce_kernel<<<(h->n_inst + 7) / 8, 256, 0, h->stream>>>(
       h->d_item_off, h->n_inst, h->d_scratch, h->d_scratch_cc, h->d_energy, h->d_ecc);
@@ -3015,20 +3057,26 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
   if (!h) return set_error(REMC_ERR_INVALID, "null handle");
   if (!h->tables_set || !h->state_set) return set_error(REMC_ERR_STATE, "tables/state not set");
   int rc = REMC_OK;
-  if (!h->d_forces) {
-    rc = dev_alloc(&h->d_forces, 3 * h->total_beads);
-    if (!rc) rc = dev_alloc(&h->d_G, (size_t)kNumAmino * kNumAmino * h->n_inst);
-    if (!rc) rc = dev_alloc(&h->d_dxi, h->n_inst);
-    if (!rc) rc = dev_alloc(&h->d_eadj, h->n_inst);
+  if (!h->d_adj_acc) {
+    // forces first, every part on a 256-byte boundary
+    auto up256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t nG = (size_t)kNumAmino * kNumAmino * h->n_inst;
+    const size_t off_f = 0;
+    const size_t off_G = up256(off_f + sizeof(float) * 3 * h->total_beads);
+    const size_t off_dxi = up256(off_G + sizeof(double) * nG);
+    const size_t off_e = up256(off_dxi + sizeof(double) * h->n_inst);
+    const size_t off_q = up256(off_e + sizeof(double) * h->n_inst);
+    h->adj_acc_bytes = off_q + 16;
+    rc = dev_alloc(&h->d_adj_acc, h->adj_acc_bytes);
     if (!rc) rc = dev_alloc(&h->d_mft, 6 * h->total_mols);
     if (rc) return rc;
+    h->d_G = reinterpret_cast<double*>(h->d_adj_acc + off_G);
+    h->d_dxi = reinterpret_cast<double*>(h->d_adj_acc + off_dxi);
+    h->d_eadj = reinterpret_cast<double*>(h->d_adj_acc + off_e);
+    h->d_adj_queue = reinterpret_cast<int*>(h->d_adj_acc + off_q);
+    h->d_forces = reinterpret_cast<float*>(h->d_adj_acc + off_f);
   }
-  REMC_CUDA_TRY(cudaMemsetAsync(h->d_forces, 0, sizeof(float) * 3 * h->total_beads, h->stream));
-  REMC_CUDA_TRY(cudaMemsetAsync(h->d_G, 0, sizeof(double) * kNumAmino * kNumAmino * h->n_inst,
-                                h->stream));
-  REMC_CUDA_TRY(cudaMemsetAsync(h->d_dxi, 0, sizeof(double) * h->n_inst, h->stream));
-  REMC_CUDA_TRY(cudaMemsetAsync(h->d_eadj, 0, sizeof(double) * h->n_inst, h->stream));
-  REMC_CUDA_TRY(cudaMemsetAsync(h->d_adj_queue, 0, sizeof(int), h->stream));
+  REMC_CUDA_TRY(cudaMemsetAsync(h->d_adj_acc, 0, h->adj_acc_bytes, h->stream));
   AdjConsts C;
   C.inv_xi = 1.0f / h->params.debye_length;
   C.inv_xi2 = C.inv_xi * C.inv_xi;
@@ -3045,7 +3093,7 @@ int remc_energy_adjoint(remc_handle* h, float* forces, double* mol_force_torque,
     per_sm = 8;
   const int grid = std::min(h->n_items, h->num_sms * per_sm);
   adj<<<grid, kTile, 0, h->stream>>>(h->d_sys, h->d_inst_sys, h->d_pos, h->d_tab, h->d_mol_start,
-                                     h->d_adj_items, h->n_items, h->d_adj_queue, h->d_forces,
+                                     h->d_items_by_cost, h->n_items, h->d_adj_queue, h->d_forces,
                                      h->d_G, h->d_dxi, h->d_eadj, consts_of(h), C);
   REMC_CUDA_TRY(cudaGetLastError());
   molecule_force_torque_kernel<<<dim3(h->n_inst, (h->mmax + 127) / 128), 128, 0, h->stream>>>(
