@@ -1519,8 +1519,7 @@ __device__ __forceinline__ void adjoint_group_crowd2(
     ey = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ey, iL, M), nM), ey);
     ez = __ffma2_rn(nL, __fadd2_rn(__ffma2_rn(ez, iL, M), nM), ez);
     const float2 r2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
-    const float2 rinv = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
-    const float2 rinv2 = __fmul2_rn(rinv, rinv);
+    const float2 rinv2 = make_float2(fast_rcp(r2.x), fast_rcp(r2.y));
     const float2 i6 = __fmul2_rn(__fmul2_rn(rinv2, rinv2), rinv2);
     float2 e = __fmul2_rn(A2, i6);
     if (R12) e = __fmul2_rn(e, i6);
