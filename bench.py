@@ -262,7 +262,9 @@ def main():
         eng.set_cluster(c_)
         sched_threads, sched_smem, chosen_by = t_, bool(m_), "--schedule"
     else:
-        sched_threads, sched_smem, _ = eng.autotune(probe_steps=min(args.block_steps, 256))
+        # probes as long as a timed block: the candidates differ by a few
+        # percent, which shorter probes do not resolve reliably
+        sched_threads, sched_smem, _ = eng.autotune(probe_steps=args.block_steps)
         chosen_by = "remc_autotune"
     stream = torch.cuda.ExternalStream(eng.stream_ptr(), device=torch.device("cuda", local))
     n_inst = eng.n_inst
