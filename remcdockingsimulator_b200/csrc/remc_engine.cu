@@ -280,7 +280,7 @@ constexpr int kRing = 64;  // proposal records held in shared memory (two halves
 // Shared-memory layout of sweep_kernel, in bytes, for capacities (nmax beads,
 // mmax molecules, lmax beads per molecule).
 struct SweepSmem {
-  size_t tab, beads, centres, trial_pos, ring, red, total;
+  size_t tab, beads, centres, trial_pos, trial_rel, ring, red, total;
   static __host__ __device__ size_t take(size_t& off, size_t bytes) {
     size_t o = off;
     off += (bytes + 15) & ~size_t(15);
@@ -297,6 +297,7 @@ struct SweepSmem {
     s.beads = take(off, beads_in_smem ? sizeof(float4) * nmax : 0);
     s.centres = take(off, mol_in_smem ? sizeof(float4) * mmax : 0);
     s.trial_pos = take(off, beads_in_smem ? sizeof(float4) * 4 * lmax : 0);
+    s.trial_rel = take(off, beads_in_smem ? sizeof(float4) * 2 * lmax : 0);
     s.ring = take(off, sizeof(StepRec) * kRing);
     s.red = take(off, sizeof(double) * 2 * csize * 2 * 32);  // [parity][rank][dE, dcc][warp]
     s.total = off;
@@ -397,14 +398,16 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
   // pair loops as loaded
   float4* const s_tpos = GB ? scratch : sm_tpos;
   // rotated relative positions of the chain's beads, computed with its trial
-  // positions by the beads' owners and installed by the same threads, so
-  // they need no shared memory: each thread reads back only what it wrote.
-  // The install writes rel without reading it, so the CTAs of a cluster,
-  // which all install the same values, cannot read one another's update.
-  // Two buffers by step parity, like the trial positions: the next step's
-  // owners (another molecule, other threads) write theirs before any
-  // barrier, while slower warps may still install from this step's
-  float4* const s_trel = scratch + 4 * (size_t)A.lmax;
+  // positions by the beads' owners and installed by the same threads (each
+  // thread reads back only what it wrote), in shared memory, or in global
+  // scratch when the beads stay in global memory. The install writes rel
+  // without reading it, so the CTAs of a cluster, which all install the same
+  // values, cannot read one another's update. Two buffers by step parity,
+  // like the trial positions: the next step's owners (another molecule,
+  // other threads) write theirs before any barrier, while slower warps may
+  // still install from this step's
+  float4* const s_trel =
+      GB ? scratch + 4 * (size_t)A.lmax : reinterpret_cast<float4*>(smem_raw + L.trial_rel);
 
   // ---- prologue: make the instance resident in shared memory
   for (int i = tid; i < kNT * kNT; i += nthr) s_tab[i] = A.tab[i];
